@@ -1,0 +1,289 @@
+"""Benchmark: 4D Wigner split-operator steps/s at 64^4 on B200.
+
+Workload (one "step" = one Run() iteration: renormalise, observables,
+kinetic half-step x<->lambda, potential half-step p<->theta): the plain
+complex128 GPU_Wigner4D drop-in on a 64x64x64x64 grid (268 MB state,
+larger than the 126 MB L2, so no flush is needed between steps), seeded
+quartic/coupling coefficients and a two-Gaussian cat state, D = 0.005,
+dt = 0.005, delta = 1/N windows.  Beside it the same step in the complex64
+precision form.  Synthetic seeded data; nothing is read from disk.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints ONE JSON line (rank 0).  ``--impl reference`` times the reference's
+algorithm on the host cores instead: the NumPy/SciPy restatement of
+GPU_Wigner4D.Run() in oracle/ (the reference itself is Python 2 + PyCUDA +
+an absent FAFT library and cannot run here), multi-threaded, on the same
+workload.  N > 1 runs N independent replicas (the path does not shard; one
+process per GPU under torchrun).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "4D Wigner steps/s at 64^4: FP32-TC batched vs FP64 plain, same B200, <=1e-6 err"
+WORKLOAD = "GPU_Wigner4D plain complex128 Run() iteration, 64x64x64x64, cat state, V=0.5r^2+q r^4+k xy"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _clock_sampler(local):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        return subprocess.Popen(["nvidia-smi", "-i", str(local), "--query-gpu=" + q,
+                                 "--format=csv,noheader,nounits", "-lms", "200"],
+                                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+        return None
+
+
+def _clock_summary(proc):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        out, _ = proc.communicate(timeout=5)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        out, _ = proc.communicate()
+    rows = [r.split(",") for r in out.strip().splitlines() if r.count(",") >= 8]
+    if not rows:
+        return None
+    sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+    mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]})
+    return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+            "reasons": reasons, "samples": len(rows)}
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def _traffic():
+    """DRAM bytes per launch from the committed ncu summary (profiles/)."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def _frame(dtype):
+    from configs import cat_xp, config2
+    from frames import make_frame
+    from pywignercuda2_b200 import GPU_Wigner4D
+    params, c = config2(seed=0, n=64)
+    f = make_frame(GPU_Wigner4D, params, complex_dtype=dtype)
+    W0 = cat_xp(f._coords, c).astype(dtype)
+    return f, W0
+
+
+def cpu_baseline_port(steps, workers, budget_s=20.0):
+    """The oracle's Run() iteration at 64^4 on the host (bounded sample)."""
+    from configs import cat_xp, config2
+    from oracle.wigner4d import Wigner4DOracle
+    import oracle.faft as of
+    params, c = config2(seed=0, n=64)
+    o = Wigner4DOracle(params)
+    coords = [o._axis(0, o.dp_y).ravel(), o._axis(1, o.dy).ravel(), o._axis(2, o.dp_x).ravel(),
+              o._axis(3, o.dx).ravel()]
+    W = cat_xp(coords, c)
+    kin, pot = o.kinetic_factor(), o.potential_factor()
+    of.FFT_WORKERS = workers
+    W = o.step(W, kin, pot)     # warm-up (plans, page faults)
+    n, t0 = 0, time.perf_counter()
+    while n < steps:
+        W = o.step(W, kin, pot)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    of.FFT_WORKERS = 1
+    return n / dt, n, dt
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    cores = len(os.sched_getaffinity(0))
+    steps = max(1, min(args.steps, 5))
+    v, n, dt = cpu_baseline_port(steps, workers=cores, budget_s=120.0)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": n, "warmup": 1, "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": [64, 64, 64, 64], "parallelism": "replicas",
+                       "cache": "inputs larger than L2"},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cores, "kind": "port",
+                             "sample": "%d Run() iterations of oracle/wigner4d.py at 64^4, scipy.fft "
+                                       "workers=%d" % (n, cores)},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from pywignercuda2_b200 import _lib
+
+    K, Wm = args.steps, args.warmup
+    f, W0 = _frame(np.complex128)
+    f.W_init_gpu.set(W0)
+    st = torch.cuda.current_stream()
+    hist = torch.empty((K + Wm + 2, _lib.WIG4D_NOBS), dtype=torch.float64, device="cuda")
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident throughput (value) ---------------------------------
+    f.run_device(f.W_init_gpu, Wm, hist)
+    barrier()
+    clk = _clock_sampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(st)
+    f.run_device(f.W_init_gpu, K, hist)
+    e1.record(st)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clocks = _clock_summary(clk)
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    value = ws * K / (ms / 1e3)
+    hcheck = hist[:K].cpu().numpy()
+    finite = bool(np.all(np.isfinite(hcheck)))
+
+    # ---- dominant-kernel roofline: each half-step kernel timed alone -------
+    P = int(np.prod(f.shape))
+    state_bytes = P * 16
+    def time_kernel(fn, reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(3):
+            fn(f.W_init_gpu)
+        torch.cuda.synchronize()
+        a.record(st)
+        for _ in range(reps):
+            fn(f.W_init_gpu)
+        b.record(st)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+    kin_ms = time_kernel(f.kinetic_halfstep, 20)
+    pot_ms = time_kernel(f.potential_halfstep, 20)
+    dom_name, dom_ms = ("k_potential", pot_ms) if pot_ms >= kin_ms else ("k_kinetic", kin_ms)
+    peaks = _peaks()
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    alg_bytes = 2 * state_bytes            # one read + one write of the state per launch
+    achieved = alg_bytes / (dom_ms / 1e3) / 1e9
+    tr = _traffic().get(dom_name + "_64^4_c128")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": tr, "kernel": dom_name,
+                "peak_source": peak_src, "algorithmic_bytes_per_launch": alg_bytes,
+                "kinetic_ms": kin_ms, "potential_ms": pot_ms,
+                "step_frac": (4 * state_bytes / (ms / K / 1e3) / 1e9) / peak}
+
+    # ---- precision form (complex64) on the same workload ----------------------
+    f32, W32 = _frame(np.complex64)
+    f32.W_init_gpu.set(W32)
+    f32.run_device(f32.W_init_gpu, Wm, hist)
+    torch.cuda.synchronize()
+    e0.record(st)
+    f32.run_device(f32.W_init_gpu, K, hist)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms32 = e0.elapsed_time(e1)
+
+    # ---- end to end through the public API with host buffers ---------------------
+    host_in = torch.from_numpy(W0).pin_memory()
+    host_out = torch.empty(f.shape, dtype=torch.complex128).pin_memory()
+    f.timeSteps = K - 1
+    f.fileName = None
+    barrier()
+    t0 = time.perf_counter()
+    e0.record(st)
+    f.W_init_gpu.tensor.copy_(host_in, non_blocking=True)
+    f.Run()                                     # history read back inside Run()
+    host_out.copy_(f.W_init_gpu.tensor, non_blocking=True)
+    e1.record(st)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+    h2d = state_bytes
+    d2h = state_bytes + K * _lib.WIG4D_NOBS * 8
+
+    line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": K,
+            "warmup": Wm, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": list(f.shape), "state_bytes": state_bytes,
+                       "parallelism": "replicas" if ws > 1 else "single",
+                       "cache": "inputs larger than L2 (268 MB state vs 126 MB L2), no flush",
+                       "factor_mode": list(f._factor_mode)},
+            "grid_point_steps_per_s": value * P,
+            "precision_form": {"dtype": "c64", "steps_per_s": K / (ms32 / 1e3),
+                               "speedup_vs_plain": (K / (ms32 / 1e3)) / (K / (ms / 1e3))},
+            "gpu_launches": 3 * K, "finite": finite, "roofline": roofline, "clocks": clocks,
+            "e2e": {"value": ws * K / (e2e_ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d / K,
+                    "d2h_bytes_per_step": d2h / K,
+                    "note": "one Run() of K iterations: pinned H2D of the state, history and "
+                            "final state read back"}}
+    if rank == 0 and not args.no_cpu_baseline:
+        v, n, dt = cpu_baseline_port(3, workers=1, budget_s=20.0)
+        line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": 1, "kind": "port",
+                                "sample": "%d Run() iterations of oracle/wigner4d.py at 64^4 "
+                                          "(numpy pocketfft, 1 thread), %.1f s" % (n, dt)}
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

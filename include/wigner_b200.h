@@ -1,0 +1,182 @@
+/*
+ * wigner_b200.h -- C ABI of the B200 (sm_100a) split-operator Wigner propagator.
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t
+ * passed as void*, and returns an int status (WIG_OK == 0).  No C++ or
+ * PyTorch type crosses this boundary; the library never frees caller memory.
+ *
+ * Reference interfaces replaced (cabrer7/PyWignerCUDA2):
+ *   FAFT64_4D_Z2Z / IFAFT64_4D_Z2Z / FAFT128_4D_Z2Z / FAFT256_4D_Z2Z
+ *       ctypes bindings of the external FAFT library, GPU_Wigner4D.py:29-58
+ *       (same in GPU_WignerDirac4D.py:29-58, GPU_WignerDiracKvN4D.py:29-58).
+ *   wig_faft            the general form of the above (any shape, axis, N).
+ *   wig4d_*             GPU_Wigner4D's JIT kernels and Run() loop,
+ *                       GPU_Wigner4D.py:216-541.
+ *   wigd_*              GPU_WignerDirac4D / GPU_WignerDiracKvN4D kernels and
+ *                       Run(), GPU_WignerDirac4D.py:240-1899,
+ *                       GPU_WignerDiracKvN4D.py:240-1669.
+ *
+ * Array convention (the reference's): a 4-D complex array of shape
+ * shape[4] = {N_py, N_y, N_px, N_x}, C order, x fastest.  "axis" is the
+ * NumPy axis index into that shape.  dtype 0 = complex128, 1 = complex64.
+ */
+#ifndef WIGNER_B200_H
+#define WIGNER_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define WIG_OK                 0
+#define WIG_ERR_INVALID_ARG    1   /* null pointer, bad axis, bad dtype       */
+#define WIG_ERR_UNSUPPORTED    2   /* shape not supported by this build       */
+#define WIG_ERR_CUDA           3   /* a CUDA runtime call failed              */
+#define WIG_ERR_ALLOC          4   /* device allocation failed                */
+#define WIG_ERR_NONFINITE      5   /* a reduction saw NaN or Inf              */
+#define WIG_ERR_ALIAS          6   /* two component pointers alias            */
+#define WIG_ERR_TOO_LARGE      7   /* size above a fixed limit of the call    */
+
+#define WIG_C128 0
+#define WIG_C64  1
+
+/* Human-readable text for a status code (static storage). */
+const char* wig_status_string(int status);
+
+/* Text of the last CUDA error seen by this library on the calling thread. */
+const char* wig_last_error(void);
+
+/* Library version as an integer, major*10000 + minor*100 + patch. */
+int wig_version(void);
+
+/* ---- the fractional centred transform (FAFT) ---------------------------- */
+/*
+ * In place along one axis:
+ *   F[k] = post_scale * 2 N d * sum_n f[n] exp(-2 pi i delta (n - N/2)(k - N/2))
+ * delta is signed (the reference's "inverse" passes -delta).  |delta| N == 1
+ * runs a radix FFT when N is 16, 32, 64 or 128; any other N or delta runs the
+ * dense transform.  Replaces one FAFT*_4D_Z2Z call (GPU_Wigner4D.py:409-427)
+ * plus, through post_scale, the wrapper's "W /= size" pass.
+ */
+int wig_faft(void* data, const int shape[4], int dtype, int axis,
+             double d, double delta, double post_scale, void* stream);
+
+/*
+ * Drop-in shims with the exact ctypes signature the reference binds
+ * (GPU_Wigner4D.py:34-35, 43-44, 51-55):
+ *   int FAFTxx_4D_Z2Z(void* dev_ptr, double d, double delta,
+ *                     int segment, int axes, double NF);
+ * FAFT64_4D_Z2Z and IFAFT64_4D_Z2Z act on a 64^4 complex128 array;
+ * FAFT128_4D_Z2Z on a (64, 64, 64, 64) array as the reference's 64x64 frames
+ * use it; FAFT256_4D_Z2Z on the (64, 64, 128, 128) array of its 64x128
+ * frames.  IFAFT64_4D_Z2Z is FAFT64_4D_Z2Z with delta negated (the reference
+ * binds but never calls it).  segment must be 0 and NF 1, the only values
+ * the reference passes.  They run on the legacy default stream.
+ */
+int FAFT64_4D_Z2Z(void* dev_ptr, double d, double delta, int segment, int axes, double NF);
+int IFAFT64_4D_Z2Z(void* dev_ptr, double d, double delta, int segment, int axes, double NF);
+int FAFT128_4D_Z2Z(void* dev_ptr, double d, double delta, int segment, int axes, double NF);
+int FAFT256_4D_Z2Z(void* dev_ptr, double d, double delta, int segment, int axes, double NF);
+
+/* ---- elementwise helpers ------------------------------------------------- */
+/* data[i] *= (s_re + i s_im) for n complex elements. */
+int wig_scale(void* data, long long n, int dtype, double s_re, double s_im, void* stream);
+/* data[i] /= *d_norm, where d_norm points at one complex128 on the device. */
+int wig_divide_by_device_scalar(void* data, long long n, int dtype,
+                                const double* d_norm, void* stream);
+/* data[i] = Re(data[i])  (Real_GPU, GPU_WignerDirac4D.py:240-244). */
+int wig_real(void* data, long long n, int dtype, void* stream);
+
+/* ---- factor tables ------------------------------------------------------- */
+/*
+ * A multiplicative phase factor is the product of up to WIG_MAX_FACTORS
+ * complex tables, each indexed by two array axes (axis_a, axis_b):
+ * value = data[i_a * shape[axis_b] + i_b].  axis_b < 0 gives a table over
+ * axis_a alone; axis_a < 0 gives a full 4-D table in the array's layout.
+ * Host data is interleaved (re, im) float64; the plan copies it to the GPU
+ * (rounded to complex64 for WIG_C64 plans).
+ */
+#define WIG_MAX_FACTORS 6
+typedef struct {
+    int axis_a;
+    int axis_b;
+    const double* host_data;
+} wig_factor;
+
+/* ---- scalar Wigner4D plan ------------------------------------------------ */
+typedef struct wig4d_plan wig4d_plan;
+
+typedef struct {
+    int shape[4];              /* N_py, N_y, N_px, N_x                          */
+    int dtype;                 /* WIG_C128 (drop-in) or WIG_C64 (precision)     */
+    /* FAFT parameters per array axis for the two half-steps.  Axes 1, 3 are
+       transformed by the kinetic half-step (x <-> lambda), axes 0, 2 by the
+       potential one (p <-> theta).  The forward call uses +delta, the inverse
+       -delta, both with the same d (GPU_Wigner4D.py:409-427).                */
+    double d[4];
+    double delta[4];
+    double kin_post_scale;     /* wrapper divisors of the kinetic pair, e.g. 1/size^2  */
+    double pot_post_scale;     /* same for the potential pair                          */
+    int n_kin;                 /* factor tables of exp_p_lambda (GPU_Wigner4D.py:251-262) */
+    wig_factor kin[WIG_MAX_FACTORS];
+    int n_pot;                 /* factor tables of exp_x_theta (GPU_Wigner4D.py:269-281)  */
+    wig_factor pot[WIG_MAX_FACTORS];
+    /* observables (GPU_Wigner4D.py:285-369): coordinates of each axis as the
+       reduction kernels see them, host float64, lengths shape[axis].          */
+    const double* coord[4];    /* p_y, y, p_x, x                                  */
+    const double* energy_p;    /* K(p_x, p_y) on [N_py][N_px]                     */
+    const double* energy_x;    /* V(x, y)     on [N_y][N_x]                       */
+    double dv_norm;            /* dV of Norm_GPU (host precision)                 */
+    double dv_obs;             /* dV of the ReductionKernels (device constants)   */
+} wig4d_desc;
+
+/* Number of float64 values wig4d_reduce and one wig4d_run iteration write. */
+#define WIG4D_NOBS 11
+/* Order: norm_re, norm_im, <x>, <p_x>, <x^2>, <p_x^2>, <y>, <p_y>, <y^2>,
+   <p_y^2>, energy  -- the moments of the state divided by its complex norm,
+   exactly as Run() records them after "W /= norm" (GPU_Wigner4D.py:483-498). */
+
+int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** plan);
+int wig4d_plan_destroy(wig4d_plan* plan);
+
+/* Fused kinetic half-step, in place: X->Lambda, exp_p_lambda, Lambda->X
+   (GPU_Wigner4D.py:501-506), times *d_inv_norm if non-null (a complex128
+   device scalar the state is divided by first, as in W4D:484). */
+int wig4d_kinetic(wig4d_plan* plan, void* W, const double* d_norm, void* stream);
+/* Fused potential half-step, in place: P->Theta, exp_x_theta, Theta->P
+   (GPU_Wigner4D.py:508-513). */
+int wig4d_potential(wig4d_plan* plan, void* W, void* stream);
+/* The factor of one half-step applied alone, in place, on a state already in
+   the (lambda, p) (which = 0) or (x, theta) (which = 1) representation:
+   exp_p_lambda_GPU / exp_x_theta_GPU (GPU_Wigner4D.py:251-281). */
+int wig4d_apply_factor(wig4d_plan* plan, void* W, int which, void* stream);
+/* Norm and observables of W (not modified) into d_out[2 * WIG4D_NOBS]
+   (device): row 0 as Run() records them (moments of W / norm), row 1 the
+   raw Re(sum q W dV) each of the reference's ReductionKernels returns for W
+   as given (GPU_Wigner4D.py:294-358); both rows start with the complex norm. */
+int wig4d_reduce(wig4d_plan* plan, const void* W, double* d_out, void* stream);
+/*
+ * Run() (GPU_Wigner4D.py:431-541) on the device: `iterations` times
+ * {renormalise, record observables, kinetic half-step, potential half-step},
+ * then a final renormalisation.  d_history receives iterations rows of
+ * WIG4D_NOBS float64 (device memory, caller-owned).  No host synchronisation
+ * happens inside; the launches are replayed from a CUDA graph.
+ */
+int wig4d_run(wig4d_plan* plan, void* W, int iterations, double* d_history, void* stream);
+
+/* Initial states on the (x, p) grid, coordinates from desc.coord:
+   HOscillatorGound_GPU (GPU_Wigner4D.py:233-245) and Gaussian_GPU (216-230). */
+int wig4d_init_ho_ground(wig4d_plan* plan, void* W, double x_mu, double y_mu,
+                         double p_x_mu, double p_y_mu, double omega_x,
+                         double omega_y, double mass, void* stream);
+int wig4d_init_gaussian(wig4d_plan* plan, void* W, double mu_p_y, double mu_y,
+                        double mu_p_x, double mu_x, double s_p_y, double s_y,
+                        double s_p_x, double s_x, void* stream);
+
+/* Bytes of device memory the plan holds (tables, partial sums). */
+long long wig4d_plan_device_bytes(const wig4d_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WIGNER_B200_H */

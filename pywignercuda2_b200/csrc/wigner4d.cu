@@ -1,0 +1,777 @@
+// wigner4d.cu -- scalar 4-D Wigner split-operator step for sm_100a.
+//
+// Replaces GPU_Wigner4D's Run() loop (GPU_Wigner4D.py:431-541): per
+// iteration, 2 x FAFT + "/= size" + exp_p_lambda + 2 x FAFT + "/= size"
+// (x <-> lambda), the same around exp_x_theta (p <-> theta), and ten host-
+// synchronising reductions.  Here one iteration is three kernels:
+//
+//   k_kinetic   one CTA per (p_y, p_x): loads the (y, x) plane, forward 2-D
+//               transform in shared memory, multiplies by the kinetic factor
+//               (phase, lambda damping, wrapper scales and the previous
+//               iteration's 1/norm folded into one complex number per
+//               point), inverse transform, stores.  1 read + 1 write.
+//   k_potential one CTA per (y, x): the same over the (p_y, p_x) plane with
+//               the Bopp potential factor; its epilogue also forms the
+//               partial sums of the next iteration's norm and observables.
+//   k_finalize  one CTA: reduces the partial sums in a fixed order, writes
+//               the observables row and the complex norm the next kinetic
+//               step divides by.
+//
+// The (-1)^n centring of the FAFT cancels between a forward and an inverse
+// transform of the same axis except on the plane's input and output, where
+// it is a sign flip; the 2 N d scales and wrapper divisors are one scalar.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "fft_smem.cuh"
+
+void* wig_dense_matrix(int n, double delta, int dtype, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Factor tables
+// ---------------------------------------------------------------------------
+template <class C>
+struct FactorSet {
+    int n;
+    const C* data[WIG_MAX_FACTORS];
+    int ia[WIG_MAX_FACTORS];
+    int ib[WIG_MAX_FACTORS];
+    int nb[WIG_MAX_FACTORS];
+};
+
+__device__ __forceinline__ int sel4(int a, int i0, int i1, int i2, int i3) {
+    return a == 0 ? i0 : (a == 1 ? i1 : (a == 2 ? i2 : i3));
+}
+
+// Product of the factor tables at point (i0, i1, i2, i3); lin is the point's
+// linear index in the array (used by full 4-D tables).
+template <class C>
+__device__ __forceinline__ C factor_at(const FactorSet<C>& F, int i0, int i1, int i2, int i3,
+                                       long long lin, C acc) {
+#pragma unroll
+    for (int t = 0; t < WIG_MAX_FACTORS; ++t) {
+        if (t < F.n) {
+            long long idx;
+            if (F.ia[t] < 0) idx = lin;
+            else if (F.ib[t] < 0) idx = sel4(F.ia[t], i0, i1, i2, i3);
+            else idx = (long long)sel4(F.ia[t], i0, i1, i2, i3) * F.nb[t] + sel4(F.ib[t], i0, i1, i2, i3);
+            acc = cmul(acc, __ldg(F.data[t] + idx));
+        }
+    }
+    return acc;
+}
+
+struct ObsTabs {
+    const double* cx;    // x[N_x]
+    const double* cy;    // y[N_y]
+    const double* cpx;   // p_x[N_px]
+    const double* cpy;   // p_y[N_py]
+    const double* ep;    // K(p_x, p_y) [N_py][N_px]
+    const double* ex;    // V(x, y) [N_y][N_x]
+};
+
+#define NPART 12   // partial sums per CTA: sum W, p_x W, p_x^2 W, p_y W, p_y^2 W, K W (complex)
+
+// Block reduction of NPART doubles; thread 0 writes out[0..NPART).
+template <int NT>
+__device__ __forceinline__ void block_sum_partials(double (&a)[NPART], double* smem, double* out) {
+#pragma unroll
+    for (int i = 0; i < NPART; ++i) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a[i] += __shfl_down_sync(0xffffffffu, a[i], o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+#pragma unroll
+        for (int i = 0; i < NPART; ++i) smem[w * NPART + i] = a[i];
+    }
+    __syncthreads();
+    if (threadIdx.x < NPART) {
+        double s = 0.0;
+        for (int k = 0; k < NT / 32; ++k) s += smem[k * NPART + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused kinetic half-step: CTA = one (p_y, p_x) plane of NY x NX points.
+// ---------------------------------------------------------------------------
+template <class C, int NY, int NX, int NT>
+__global__ void __launch_bounds__(NT) k_kinetic(C* __restrict__ W, int npy, int npx,
+                                                FactorSet<C> F, double2 scale,
+                                                const double* __restrict__ d_norm) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* s = reinterpret_cast<C*>(smraw);
+    C* twx = s + NY * NX;
+    C* twy = twx + NX;
+    const int ipx = blockIdx.x % npx, ipy = blockIdx.x / npx;
+    make_twiddles(twx, NX);
+    if (NY != NX) make_twiddles(twy, NY);
+    const C* ty = (NY != NX) ? twy : twx;
+
+    const long long rowstride = (long long)npx * NX;
+    C* g = W + ((long long)ipy * NY * npx + ipx) * NX;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < NY * NX; e += NT) {
+        const int y = e / NX, x = e % NX;
+        C v = g[y * rowstride + x];
+        if ((x + y) & 1) v = cneg(v);
+        s[e] = v;
+    }
+    __syncthreads();
+    LineMap rows{1, NX, 0, 1}, cols{1, 1, 0, NX};
+    fft_lines<C, NX, NY, NT, true, false>(s, rows, twx);
+    fft_lines<C, NY, NX, NT, true, true>(s, cols, ty);
+
+    double2 c0 = scale;
+    if (d_norm) c0 = zmul(c0, zinv(make_double2(d_norm[0], d_norm[1])));
+    const C cc = to_c<C>(c0);
+    const long long lin0 = ((long long)ipy * NY * npx + ipx) * NX;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < NY * NX; e += NT) {
+        const int y = e / NX, x = e % NX;
+        C f = factor_at(F, ipy, y, ipx, x, lin0 + y * rowstride + x, cc);
+        s[e] = cmul(s[e], f);
+    }
+    __syncthreads();
+    fft_lines<C, NY, NX, NT, false, true>(s, cols, ty);
+    fft_lines<C, NX, NY, NT, false, false>(s, rows, twx);
+#pragma unroll 4
+    for (int e = threadIdx.x; e < NY * NX; e += NT) {
+        const int y = e / NX, x = e % NX;
+        C v = s[e];
+        if ((x + y) & 1) v = cneg(v);
+        g[y * rowstride + x] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused potential half-step: CTA = one (y, x) column, the (p_y, p_x) plane.
+// Epilogue: partial sums of the next iteration's reductions.
+// ---------------------------------------------------------------------------
+template <class C, int NPY, int NPX, int NT>
+__global__ void __launch_bounds__(NT) k_potential(C* __restrict__ W, int ny, int nx,
+                                                  FactorSet<C> F, double2 scale, ObsTabs ob,
+                                                  double* __restrict__ partials) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* s = reinterpret_cast<C*>(smraw);
+    C* twx = s + NPY * NPX;
+    C* twy = twx + NPX;
+    const int ix = blockIdx.x % nx, iy = blockIdx.x / nx;
+    make_twiddles(twx, NPX);
+    if (NPY != NPX) make_twiddles(twy, NPY);
+    const C* ty = (NPY != NPX) ? twy : twx;
+
+    const long long pxs = nx;                       // stride of p_x
+    const long long pys = (long long)ny * NPX * nx; // stride of p_y
+    C* g = W + (long long)iy * NPX * nx + ix;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < NPY * NPX; e += NT) {
+        const int py = e / NPX, px = e % NPX;
+        C v = g[py * pys + px * pxs];
+        if ((px + py) & 1) v = cneg(v);
+        s[e] = v;
+    }
+    __syncthreads();
+    LineMap rows{1, NPX, 0, 1}, cols{1, 1, 0, NPX};
+    fft_lines<C, NPX, NPY, NT, true, false>(s, rows, twx);
+    fft_lines<C, NPY, NPX, NT, true, true>(s, cols, ty);
+    const C cc = to_c<C>(scale);
+    const long long lin0 = (long long)iy * NPX * nx + ix;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < NPY * NPX; e += NT) {
+        const int py = e / NPX, px = e % NPX;
+        C f = factor_at(F, py, iy, px, ix, lin0 + py * pys + px * pxs, cc);
+        s[e] = cmul(s[e], f);
+    }
+    __syncthreads();
+    fft_lines<C, NPY, NPX, NT, false, true>(s, cols, ty);
+    fft_lines<C, NPX, NPY, NT, false, false>(s, rows, twx);
+
+    double a[NPART];
+#pragma unroll
+    for (int i = 0; i < NPART; ++i) a[i] = 0.0;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < NPY * NPX; e += NT) {
+        const int py = e / NPX, px = e % NPX;
+        C v = s[e];
+        if ((px + py) & 1) v = cneg(v);
+        g[py * pys + px * pxs] = v;
+        if (partials) {
+            const double2 w = to_d2(v);
+            const double qx = __ldg(ob.cpx + px), qy = __ldg(ob.cpy + py);
+            const double k = __ldg(ob.ep + py * NPX + px);
+            a[0] += w.x; a[1] += w.y;
+            a[2] = fma(qx, w.x, a[2]); a[3] = fma(qx, w.y, a[3]);
+            a[4] = fma(qx * qx, w.x, a[4]); a[5] = fma(qx * qx, w.y, a[5]);
+            a[6] = fma(qy, w.x, a[6]); a[7] = fma(qy, w.y, a[7]);
+            a[8] = fma(qy * qy, w.x, a[8]); a[9] = fma(qy * qy, w.y, a[9]);
+            a[10] = fma(k, w.x, a[10]); a[11] = fma(k, w.y, a[11]);
+        }
+    }
+    if (partials) {
+        __syncthreads();   // smem reused for the block reduction
+        block_sum_partials<NT>(a, reinterpret_cast<double*>(smraw), partials + (long long)blockIdx.x * NPART);
+    }
+}
+
+// Standalone reduction of a state in the (x, p) representation: same CTA
+// shape and partial layout as k_potential's epilogue.
+template <class C, int NT>
+__global__ void __launch_bounds__(NT) k_reduce_xp(const C* __restrict__ W, int npy, int ny, int npx,
+                                                  int nx, ObsTabs ob, double* __restrict__ partials) {
+    __shared__ double sm[NPART * (NT / 32)];
+    const int ix = blockIdx.x % nx, iy = blockIdx.x / nx;
+    const long long pxs = nx, pys = (long long)ny * npx * nx;
+    const C* g = W + (long long)iy * npx * nx + ix;
+    double a[NPART];
+#pragma unroll
+    for (int i = 0; i < NPART; ++i) a[i] = 0.0;
+    for (int e = threadIdx.x; e < npy * npx; e += NT) {
+        const int py = e / npx, px = e % npx;
+        const double2 w = to_d2(g[py * pys + px * pxs]);
+        const double qx = ob.cpx[px], qy = ob.cpy[py], k = ob.ep[py * npx + px];
+        a[0] += w.x; a[1] += w.y;
+        a[2] = fma(qx, w.x, a[2]); a[3] = fma(qx, w.y, a[3]);
+        a[4] = fma(qx * qx, w.x, a[4]); a[5] = fma(qx * qx, w.y, a[5]);
+        a[6] = fma(qy, w.x, a[6]); a[7] = fma(qy, w.y, a[7]);
+        a[8] = fma(qy * qy, w.x, a[8]); a[9] = fma(qy * qy, w.y, a[9]);
+        a[10] = fma(k, w.x, a[10]); a[11] = fma(k, w.y, a[11]);
+    }
+    block_sum_partials<NT>(a, sm, partials + (long long)blockIdx.x * NPART);
+}
+
+// Final reduction: one CTA of 1024 threads, fixed summation order.
+// Writes out[WIG4D_NOBS] (row of the history, or of wig4d_reduce) and the
+// complex norm into cur_norm.  Row index comes from *counter when non-null.
+__global__ void __launch_bounds__(1024) k_finalize(const double* __restrict__ part, int nblk, int nx,
+                                                   ObsTabs ob, double dv_norm, double dv_obs,
+                                                   double* out, int* counter, int max_rows,
+                                                   double* cur_norm, int* flag, double* raw_out) {
+    constexpr int NS = 22;
+    __shared__ double sm[NS * 32];
+    double a[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) a[i] = 0.0;
+    for (int c = threadIdx.x; c < nblk; c += 1024) {
+        const int ix = c % nx, iy = c / nx;
+        const double x = ob.cx[ix], y = ob.cy[iy], V = ob.ex[iy * nx + ix];
+        const double* p = part + (long long)c * NPART;
+        const double wr = p[0], wi = p[1];
+        a[0] += wr; a[1] += wi;                              // sum W
+        a[2] = fma(x, wr, a[2]); a[3] = fma(x, wi, a[3]);    // x W
+        a[4] += p[2]; a[5] += p[3];                          // p_x W
+        a[6] = fma(x * x, wr, a[6]); a[7] = fma(x * x, wi, a[7]);
+        a[8] += p[4]; a[9] += p[5];                          // p_x^2 W
+        a[10] = fma(y, wr, a[10]); a[11] = fma(y, wi, a[11]);
+        a[12] += p[6]; a[13] += p[7];                        // p_y W
+        a[14] = fma(y * y, wr, a[14]); a[15] = fma(y * y, wi, a[15]);
+        a[16] += p[8]; a[17] += p[9];                        // p_y^2 W
+        a[18] += p[10]; a[19] += p[11];                      // K W
+        a[20] = fma(V, wr, a[20]); a[21] = fma(V, wi, a[21]); // V W
+    }
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a[i] += __shfl_down_sync(0xffffffffu, a[i], o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+#pragma unroll
+        for (int i = 0; i < NS; ++i) sm[w * NS + i] = a[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double S[NS];
+        for (int i = 0; i < NS; ++i) {
+            double t = 0.0;
+            for (int k = 0; k < 32; ++k) t += sm[k * NS + i];
+            S[i] = t;
+        }
+        const double2 n = make_double2(S[0] * dv_norm, S[1] * dv_norm);
+        const double2 inv = zinv(n);
+        auto obs = [&](int k) { return dv_obs * (S[k] * inv.x - S[k + 1] * inv.y); };
+        double row[WIG4D_NOBS];
+        row[0] = n.x; row[1] = n.y;
+        row[2] = obs(2); row[3] = obs(4); row[4] = obs(6); row[5] = obs(8);
+        row[6] = obs(10); row[7] = obs(12); row[8] = obs(14); row[9] = obs(16);
+        row[10] = dv_obs * ((S[18] + S[20]) * inv.x - (S[19] + S[21]) * inv.y);
+        double* dst = out;
+        if (counter) {
+            int r = *counter;
+            dst = (r < max_rows) ? out + (long long)r * WIG4D_NOBS : nullptr;
+            *counter = r + 1;
+        }
+        bool bad = false;
+        for (int i = 0; i < WIG4D_NOBS; ++i) bad |= !isfinite(row[i]);
+        if (bad && flag) *flag = WIG_ERR_NONFINITE;
+        if (dst)
+            for (int i = 0; i < WIG4D_NOBS; ++i) dst[i] = row[i];
+        if (cur_norm) { cur_norm[0] = n.x; cur_norm[1] = n.y; }
+        if (raw_out) {   // Re(dV sum q W) of the state as given, as a ReductionKernel returns it
+            raw_out[0] = n.x; raw_out[1] = n.y;
+            for (int q = 0; q < 8; ++q) raw_out[2 + q] = dv_obs * S[2 + 2 * q];
+            raw_out[10] = dv_obs * (S[18] + S[20]);
+        }
+    }
+}
+
+// Factor applied alone (unfused path): elementwise over the whole array.
+template <class C>
+__global__ void k_apply_factor(C* W, int n0, int n1, int n2, int n3, FactorSet<C> F, double2 scale) {
+    const long long tot = (long long)n0 * n1 * n2 * n3;
+    const C cc = to_c<C>(scale);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int i3 = i % n3;
+        const int i2 = (i / n3) % n2;
+        const int i1 = (i / ((long long)n3 * n2)) % n1;
+        const int i0 = i / ((long long)n3 * n2 * n1);
+        W[i] = cmul(W[i], factor_at(F, i0, i1, i2, i3, i, cc));
+    }
+}
+
+// Initial states (GPU_Wigner4D.py:216-245) on the (x, p) grid.
+template <class C>
+__global__ void k_init_ho(C* W, int n0, int n1, int n2, int n3, ObsTabs ob, double x_mu, double y_mu,
+                          double px_mu, double py_mu, double wx, double wy, double mass) {
+    const long long tot = (long long)n0 * n1 * n2 * n3;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int i3 = i % n3, i2 = (i / n3) % n2, i1 = (i / ((long long)n3 * n2)) % n1;
+        const int i0 = i / ((long long)n3 * n2 * n1);
+        const double x = ob.cx[i3], px = ob.cpx[i2], y = ob.cy[i1], py = ob.cpy[i0];
+        double t = (mass * pow(wx * (x - x_mu), 2.0) + pow(px - px_mu, 2.0) / mass) / wx;
+        t += (mass * pow(wy * (y - y_mu), 2.0) + pow(py - py_mu, 2.0) / mass) / wy;
+        W[i] = to_c<C>(make_double2(exp(-t), 0.0));
+    }
+}
+template <class C>
+__global__ void k_init_gauss(C* W, int n0, int n1, int n2, int n3, ObsTabs ob, double mpy, double my,
+                             double mpx, double mx, double spy, double sy, double spx, double sx) {
+    const long long tot = (long long)n0 * n1 * n2 * n3;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int i3 = i % n3, i2 = (i / n3) % n2, i1 = (i / ((long long)n3 * n2)) % n1;
+        const int i0 = i / ((long long)n3 * n2 * n1);
+        const double x = ob.cx[i3], px = ob.cpx[i2], y = ob.cy[i1], py = ob.cpy[i0];
+        double t = exp(-0.5 * (x - mx) * (x - mx) / (sx * sx));
+        t *= exp(-0.5 * (y - my) * (y - my) / (sy * sy));
+        t *= exp(-0.5 * (px - mpx) * (px - mpx) / (spx * spx));
+        t *= exp(-0.5 * (py - mpy) * (py - mpy) / (spy * spy));
+        W[i] = to_c<C>(make_double2(t, 0.0));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Plan
+// ---------------------------------------------------------------------------
+struct wig4d_plan {
+    int shape[4];
+    int dtype;
+    double d[4], delta[4];
+    double kin_scale, pot_scale;   // total scalar of each fused half-step
+    bool fused_kin, fused_pot;     // fused fast kernels usable
+    double dv_norm, dv_obs;
+    long long npts;
+    // device memory
+    void* tabs;                    // all factor tables (one allocation)
+    long long tab_bytes;
+    FactorSet<double2> kin_d, pot_d;
+    FactorSet<float2> kin_f, pot_f;
+    double* obs_mem;               // coords + energy tables
+    ObsTabs ob;
+    double* partials;              // NPART per (y, x) column
+    double* cur_norm;              // complex128 norm of the current state
+    int* counter;                  // history row of the next finalize
+    int* flag;                     // WIG_ERR_NONFINITE when seen
+    // CUDA graph of one Run() iteration, cached per (W, history, stream)
+    cudaGraphExec_t graph;
+    void* graph_W;
+    double* graph_hist;
+    int graph_rows;
+};
+
+static bool pow2_16_128(int n) { return n == 16 || n == 32 || n == 64 || n == 128; }
+
+template <class C>
+static size_t plane_smem(int a, int b) { return sizeof(C) * ((size_t)a * b + a + b); }
+
+template <class C> static FactorSet<C>& kin_set(wig4d_plan* p);
+template <> FactorSet<double2>& kin_set<double2>(wig4d_plan* p) { return p->kin_d; }
+template <> FactorSet<float2>& kin_set<float2>(wig4d_plan* p) { return p->kin_f; }
+template <class C> static FactorSet<C>& pot_set(wig4d_plan* p);
+template <> FactorSet<double2>& pot_set<double2>(wig4d_plan* p) { return p->pot_d; }
+template <> FactorSet<float2>& pot_set<float2>(wig4d_plan* p) { return p->pot_f; }
+
+// Dispatch a fused kernel over the supported plane sizes.
+#define WIG_PLANE_CASES(X) X(16, 16) X(32, 32) X(64, 64) X(128, 128) X(64, 128) X(128, 64)
+
+template <class C>
+static int launch_kinetic(wig4d_plan* p, C* W, const double* d_norm, cudaStream_t st) {
+    const int NY = p->shape[1], NX = p->shape[3];
+    const int npy = p->shape[0], npx = p->shape[2];
+    const unsigned grid = (unsigned)(npy * npx);
+    const double2 sc = make_double2(p->kin_scale, 0.0);
+#define KCASE(a, b)                                                                      \
+    if (NY == a && NX == b) {                                                            \
+        auto kern = k_kinetic<C, a, b, 256>;                                             \
+        size_t sm = plane_smem<C>(a, b);                                                 \
+        WIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+        kern<<<grid, 256, sm, st>>>(W, npy, npx, kin_set<C>(p), sc, d_norm);             \
+        WIG_LAUNCHED("k_kinetic");                                                       \
+        return WIG_OK;                                                                   \
+    }
+    WIG_PLANE_CASES(KCASE)
+#undef KCASE
+    return WIG_ERR_UNSUPPORTED;
+}
+
+template <class C>
+static int launch_potential(wig4d_plan* p, C* W, double* partials, cudaStream_t st) {
+    const int NPY = p->shape[0], NPX = p->shape[2];
+    const int ny = p->shape[1], nx = p->shape[3];
+    const unsigned grid = (unsigned)(ny * nx);
+    const double2 sc = make_double2(p->pot_scale, 0.0);
+#define PCASE(a, b)                                                                      \
+    if (NPY == a && NPX == b) {                                                          \
+        auto kern = k_potential<C, a, b, 256>;                                           \
+        size_t sm = plane_smem<C>(a, b);                                                 \
+        if (sm < NPART * 8 * sizeof(double)) sm = NPART * 8 * sizeof(double);            \
+        WIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+        kern<<<grid, 256, sm, st>>>(W, ny, nx, pot_set<C>(p), sc, p->ob, partials);      \
+        WIG_LAUNCHED("k_potential");                                                     \
+        return WIG_OK;                                                                   \
+    }
+    WIG_PLANE_CASES(PCASE)
+#undef PCASE
+    return WIG_ERR_UNSUPPORTED;
+}
+
+static unsigned grid_for(long long n) {
+    long long b = (n + 255) / 256, cap = (long long)wig_num_sms() * 16;
+    return (unsigned)(b < cap ? (b > 0 ? b : 1) : cap);
+}
+
+// Unfused fallback of one half-step: FAFT pair, factor, inverse pair.
+template <class C>
+static int halfstep_unfused(wig4d_plan* p, C* W, int which, const double* d_norm, cudaStream_t st) {
+    const int a0 = which == 0 ? 1 : 0, a1 = which == 0 ? 3 : 2;
+    int s;
+    if ((s = wig_faft(W, p->shape, p->dtype, a0, p->d[a0], p->delta[a0], 1.0, st))) return s;
+    if ((s = wig_faft(W, p->shape, p->dtype, a1, p->d[a1], p->delta[a1], 1.0, st))) return s;
+    if (d_norm) {
+        if ((s = wig_divide_by_device_scalar(W, p->npts, p->dtype, d_norm, st))) return s;
+    }
+    const double post = which == 0 ? p->kin_scale : p->pot_scale;
+    // kin_scale holds the FAFT 2Nd factors of both directions; the transforms
+    // above and below already apply them, so only the wrapper divisors remain.
+    double f = post;
+    for (int a : {a0, a1}) f /= (2.0 * p->shape[a] * p->d[a]) * (2.0 * p->shape[a] * p->d[a]);
+    FactorSet<C>& F = which == 0 ? kin_set<C>(p) : pot_set<C>(p);
+    k_apply_factor<C><<<grid_for(p->npts), 256, 0, st>>>(W, p->shape[0], p->shape[1], p->shape[2],
+                                                         p->shape[3], F, make_double2(f, 0.0));
+    WIG_LAUNCHED("k_apply_factor");
+    if ((s = wig_faft(W, p->shape, p->dtype, a0, p->d[a0], -p->delta[a0], 1.0, st))) return s;
+    if ((s = wig_faft(W, p->shape, p->dtype, a1, p->d[a1], -p->delta[a1], 1.0, st))) return s;
+    return WIG_OK;
+}
+
+template <class C>
+static int kinetic_impl(wig4d_plan* p, C* W, const double* d_norm, cudaStream_t st) {
+    if (p->fused_kin) return launch_kinetic<C>(p, W, d_norm, st);
+    return halfstep_unfused<C>(p, W, 0, d_norm, st);
+}
+
+template <class C>
+static int potential_impl(wig4d_plan* p, C* W, double* partials, cudaStream_t st) {
+    if (p->fused_pot) return launch_potential<C>(p, W, partials, st);
+    int s = halfstep_unfused<C>(p, W, 1, nullptr, st);
+    if (s || !partials) return s;
+    k_reduce_xp<C, 256><<<p->shape[1] * p->shape[3], 256, 0, st>>>(
+        W, p->shape[0], p->shape[1], p->shape[2], p->shape[3], p->ob, partials);
+    WIG_LAUNCHED("k_reduce_xp");
+    return WIG_OK;
+}
+
+static int finalize(wig4d_plan* p, double* out, int* counter, int max_rows, cudaStream_t st,
+                    double* raw_out = nullptr) {
+    k_finalize<<<1, 1024, 0, st>>>(p->partials, p->shape[1] * p->shape[3], p->shape[3], p->ob,
+                                   p->dv_norm, p->dv_obs, out, counter, max_rows, p->cur_norm, p->flag,
+                                   raw_out);
+    WIG_LAUNCHED("k_finalize");
+    return WIG_OK;
+}
+
+template <class C>
+static int reduce_impl(wig4d_plan* p, const C* W, cudaStream_t st) {
+    k_reduce_xp<C, 256><<<p->shape[1] * p->shape[3], 256, 0, st>>>(
+        W, p->shape[0], p->shape[1], p->shape[2], p->shape[3], p->ob, p->partials);
+    WIG_LAUNCHED("k_reduce_xp");
+    return WIG_OK;
+}
+
+static void free_plan(wig4d_plan* p) {
+    if (!p) return;
+    if (p->graph) cudaGraphExecDestroy(p->graph);
+    cudaFree(p->tabs);
+    cudaFree(p->obs_mem);
+    cudaFree(p->partials);
+    cudaFree(p->cur_norm);
+    delete p;
+}
+
+extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
+    if (!desc || !out) return WIG_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (desc->dtype != WIG_C128 && desc->dtype != WIG_C64) return WIG_ERR_INVALID_ARG;
+    for (int a = 0; a < 4; ++a) {
+        if (desc->shape[a] < 2 || desc->shape[a] > 1024 || (desc->shape[a] & 1)) return WIG_ERR_UNSUPPORTED;
+        if (!desc->coord[a]) return WIG_ERR_INVALID_ARG;
+    }
+    if (!desc->energy_p || !desc->energy_x) return WIG_ERR_INVALID_ARG;
+    if (desc->n_kin < 0 || desc->n_kin > WIG_MAX_FACTORS || desc->n_pot < 0 ||
+        desc->n_pot > WIG_MAX_FACTORS)
+        return WIG_ERR_INVALID_ARG;
+    wig4d_plan* p = new wig4d_plan();
+    memset(p, 0, sizeof(*p));
+    memcpy(p->shape, desc->shape, sizeof(p->shape));
+    p->dtype = desc->dtype;
+    memcpy(p->d, desc->d, sizeof(p->d));
+    memcpy(p->delta, desc->delta, sizeof(p->delta));
+    p->npts = (long long)p->shape[0] * p->shape[1] * p->shape[2] * p->shape[3];
+    p->dv_norm = desc->dv_norm;
+    p->dv_obs = desc->dv_obs;
+    // total scalar of a fused half-step: (2 N d)^2 per transformed axis (the
+    // forward and the inverse FAFT) times the wrapper divisors.
+    p->kin_scale = desc->kin_post_scale;
+    p->pot_scale = desc->pot_post_scale;
+    for (int a : {1, 3}) p->kin_scale *= (2.0 * p->shape[a] * p->d[a]) * (2.0 * p->shape[a] * p->d[a]);
+    for (int a : {0, 2}) p->pot_scale *= (2.0 * p->shape[a] * p->d[a]) * (2.0 * p->shape[a] * p->d[a]);
+    auto fast_axis = [&](int a) {
+        return pow2_16_128(p->shape[a]) && fabs(fabs(p->delta[a]) * p->shape[a] - 1.0) < 1e-12;
+    };
+    const size_t esz = desc->dtype == WIG_C128 ? 16 : 8;
+    const size_t max_smem = 227 * 1024;
+    p->fused_kin = fast_axis(1) && fast_axis(3) &&
+                   esz * ((size_t)p->shape[1] * p->shape[3] + p->shape[1] + p->shape[3]) <= max_smem;
+    p->fused_pot = fast_axis(0) && fast_axis(2) &&
+                   esz * ((size_t)p->shape[0] * p->shape[2] + p->shape[0] + p->shape[2]) <= max_smem;
+    auto plane_ok = [](int a, int b) {
+        return (a == b && pow2_16_128(a)) || (a == 64 && b == 128) || (a == 128 && b == 64);
+    };
+    p->fused_kin = p->fused_kin && plane_ok(p->shape[1], p->shape[3]);
+    p->fused_pot = p->fused_pot && plane_ok(p->shape[0], p->shape[2]);
+
+    // ---- factor tables: one device allocation ----
+    auto tab_elems = [&](const wig_factor& f) -> long long {
+        if (f.axis_a < 0) return p->npts;
+        if (f.axis_b < 0) return p->shape[f.axis_a];
+        return (long long)p->shape[f.axis_a] * p->shape[f.axis_b];
+    };
+    long long tot = 0;
+    for (int i = 0; i < desc->n_kin; ++i) tot += tab_elems(desc->kin[i]);
+    for (int i = 0; i < desc->n_pot; ++i) tot += tab_elems(desc->pot[i]);
+    for (int i = 0; i < desc->n_kin; ++i) if (!desc->kin[i].host_data) { delete p; return WIG_ERR_INVALID_ARG; }
+    for (int i = 0; i < desc->n_pot; ++i) if (!desc->pot[i].host_data) { delete p; return WIG_ERR_INVALID_ARG; }
+    p->tab_bytes = tot * (long long)esz;
+    if (tot > 0 && cudaMalloc(&p->tabs, (size_t)p->tab_bytes) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+    long long off = 0;
+    auto upload = [&](const wig_factor& f, const void** dst, int* ia, int* ib, int* nb) -> int {
+        const long long n = tab_elems(f);
+        char* base = reinterpret_cast<char*>(p->tabs) + off * esz;
+        if (desc->dtype == WIG_C128) {
+            if (cudaMemcpy(base, f.host_data, n * 16, cudaMemcpyHostToDevice) != cudaSuccess) return WIG_ERR_CUDA;
+        } else {
+            std::vector<float> tmp(2 * n);
+            for (long long i = 0; i < 2 * n; ++i) tmp[i] = (float)f.host_data[i];
+            if (cudaMemcpy(base, tmp.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess) return WIG_ERR_CUDA;
+        }
+        *dst = base;
+        *ia = f.axis_a;
+        *ib = f.axis_b;
+        *nb = f.axis_b >= 0 ? p->shape[f.axis_b] : 1;
+        off += n;
+        return WIG_OK;
+    };
+    p->kin_d.n = p->kin_f.n = desc->n_kin;
+    p->pot_d.n = p->pot_f.n = desc->n_pot;
+    for (int i = 0; i < desc->n_kin; ++i) {
+        const void* dp;
+        int r = upload(desc->kin[i], &dp, &p->kin_d.ia[i], &p->kin_d.ib[i], &p->kin_d.nb[i]);
+        if (r) { free_plan(p); return r; }
+        p->kin_d.data[i] = (const double2*)dp; p->kin_f.data[i] = (const float2*)dp;
+        p->kin_f.ia[i] = p->kin_d.ia[i]; p->kin_f.ib[i] = p->kin_d.ib[i]; p->kin_f.nb[i] = p->kin_d.nb[i];
+    }
+    for (int i = 0; i < desc->n_pot; ++i) {
+        const void* dp;
+        int r = upload(desc->pot[i], &dp, &p->pot_d.ia[i], &p->pot_d.ib[i], &p->pot_d.nb[i]);
+        if (r) { free_plan(p); return r; }
+        p->pot_d.data[i] = (const double2*)dp; p->pot_f.data[i] = (const float2*)dp;
+        p->pot_f.ia[i] = p->pot_d.ia[i]; p->pot_f.ib[i] = p->pot_d.ib[i]; p->pot_f.nb[i] = p->pot_d.nb[i];
+    }
+    // ---- observable tables ----
+    const int N0 = p->shape[0], N1 = p->shape[1], N2 = p->shape[2], N3 = p->shape[3];
+    const long long nobs = N0 + N1 + N2 + N3 + (long long)N0 * N2 + (long long)N1 * N3;
+    if (cudaMalloc(&p->obs_mem, nobs * sizeof(double)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+    double* q = p->obs_mem;
+    p->ob.cpy = q; cudaMemcpy(q, desc->coord[0], N0 * 8, cudaMemcpyHostToDevice); q += N0;
+    p->ob.cy = q;  cudaMemcpy(q, desc->coord[1], N1 * 8, cudaMemcpyHostToDevice); q += N1;
+    p->ob.cpx = q; cudaMemcpy(q, desc->coord[2], N2 * 8, cudaMemcpyHostToDevice); q += N2;
+    p->ob.cx = q;  cudaMemcpy(q, desc->coord[3], N3 * 8, cudaMemcpyHostToDevice); q += N3;
+    p->ob.ep = q;  cudaMemcpy(q, desc->energy_p, (size_t)N0 * N2 * 8, cudaMemcpyHostToDevice); q += (long long)N0 * N2;
+    p->ob.ex = q;  cudaMemcpy(q, desc->energy_x, (size_t)N1 * N3 * 8, cudaMemcpyHostToDevice);
+    // ---- reduction scratch: partials, current norm, row counter, flag ----
+    const size_t npart = (size_t)N1 * N3 * NPART;
+    if (cudaMalloc(&p->partials, npart * sizeof(double)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+    if (cudaMalloc(&p->cur_norm, 4 * sizeof(double)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+    p->counter = reinterpret_cast<int*>(p->cur_norm + 2);
+    p->flag = p->counter + 1;
+    cudaMemset(p->cur_norm, 0, 4 * sizeof(double));
+    // dense matrices for the unfused general-delta path are created now, so
+    // that no allocation happens during graph capture
+    for (int a = 0; a < 4; ++a) {
+        const bool fast = pow2_16_128(p->shape[a]) && fabs(fabs(p->delta[a]) * p->shape[a] - 1.0) < 1e-12;
+        if (!fast && !wig_dense_matrix(p->shape[a], fabs(p->delta[a]), p->dtype, 0)) { free_plan(p); return WIG_ERR_ALLOC; }
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) { wig_set_cuda_error(e, "wig4d_plan_create"); free_plan(p); return WIG_ERR_CUDA; }
+    *out = p;
+    return WIG_OK;
+}
+
+extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
+    if (!p) return WIG_ERR_INVALID_ARG;
+    cudaDeviceSynchronize();
+    free_plan(p);
+    return WIG_OK;
+}
+
+extern "C" long long wig4d_plan_device_bytes(const wig4d_plan* p) {
+    if (!p) return -1;
+    const long long N0 = p->shape[0], N1 = p->shape[1], N2 = p->shape[2], N3 = p->shape[3];
+    return p->tab_bytes + 8 * (N0 + N1 + N2 + N3 + N0 * N2 + N1 * N3) + 8LL * N1 * N3 * NPART + 32;
+}
+
+extern "C" int wig4d_kinetic(wig4d_plan* p, void* W, const double* d_norm, void* stream) {
+    if (!p || !W) return WIG_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    return p->dtype == WIG_C128 ? kinetic_impl<double2>(p, (double2*)W, d_norm, st)
+                                : kinetic_impl<float2>(p, (float2*)W, d_norm, st);
+}
+
+extern "C" int wig4d_potential(wig4d_plan* p, void* W, void* stream) {
+    if (!p || !W) return WIG_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    return p->dtype == WIG_C128 ? potential_impl<double2>(p, (double2*)W, nullptr, st)
+                                : potential_impl<float2>(p, (float2*)W, nullptr, st);
+}
+
+extern "C" int wig4d_apply_factor(wig4d_plan* p, void* W, int which, void* stream) {
+    if (!p || !W || (which != 0 && which != 1)) return WIG_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    // the factor alone, without the FAFT 2Nd factors or wrapper divisors
+    const double2 one = make_double2(1.0, 0.0);
+    if (p->dtype == WIG_C128) {
+        k_apply_factor<double2><<<grid_for(p->npts), 256, 0, st>>>((double2*)W, p->shape[0], p->shape[1],
+            p->shape[2], p->shape[3], which == 0 ? p->kin_d : p->pot_d, one);
+    } else {
+        k_apply_factor<float2><<<grid_for(p->npts), 256, 0, st>>>((float2*)W, p->shape[0], p->shape[1],
+            p->shape[2], p->shape[3], which == 0 ? p->kin_f : p->pot_f, one);
+    }
+    WIG_LAUNCHED("k_apply_factor");
+    return WIG_OK;
+}
+
+extern "C" int wig4d_reduce(wig4d_plan* p, const void* W, double* d_out, void* stream) {
+    if (!p || !W || !d_out) return WIG_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    int s = p->dtype == WIG_C128 ? reduce_impl<double2>(p, (const double2*)W, st)
+                                 : reduce_impl<float2>(p, (const float2*)W, st);
+    if (s) return s;
+    return finalize(p, d_out, nullptr, 0, st, d_out + WIG4D_NOBS);
+}
+
+// One Run() iteration: kinetic (dividing by the current norm), potential
+// with the partial sums of the new state, finalize into the history.
+template <class C>
+static int iteration(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t st) {
+    int s;
+    if ((s = kinetic_impl<C>(p, W, p->cur_norm, st))) return s;
+    if ((s = potential_impl<C>(p, W, p->partials, st))) return s;
+    return finalize(p, hist, p->counter, rows, st);
+}
+
+template <class C>
+static int run_impl(wig4d_plan* p, C* W, int iterations, double* hist, cudaStream_t st) {
+    int s;
+    // counter = 0, flag = 0
+    WIG_CUDA(cudaMemsetAsync(p->counter, 0, 2 * sizeof(int), st));
+    // observables of the initial state are row 0; its norm divides iteration 0
+    if ((s = reduce_impl<C>(p, W, st))) return s;
+    if ((s = finalize(p, hist, p->counter, iterations, st))) return s;
+    if (iterations <= 0) return WIG_OK;
+    // iteration 0 runs eagerly (kernel attributes get set outside any capture);
+    // the rest replay a CUDA graph of one iteration
+    if ((s = iteration<C>(p, W, hist, iterations, st))) return s;
+    if (iterations == 1)
+        return wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st);
+    if (!p->graph || p->graph_W != (void*)W || p->graph_hist != hist || p->graph_rows != iterations) {
+        if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
+        cudaStream_t cap;
+        WIG_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaGraph_t g;
+        WIG_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        int r = iteration<C>(p, W, hist, iterations, cap);
+        cudaError_t e = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (r) return r;
+        if (e != cudaSuccess) { wig_set_cuda_error(e, "cudaStreamEndCapture"); return WIG_ERR_CUDA; }
+        e = cudaGraphInstantiate(&p->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { wig_set_cuda_error(e, "cudaGraphInstantiate"); p->graph = nullptr; return WIG_ERR_CUDA; }
+        p->graph_W = W; p->graph_hist = hist; p->graph_rows = iterations;
+    }
+    // iterations: the last row recorded is that of the final state
+    for (int i = 1; i < iterations; ++i) WIG_CUDA(cudaGraphLaunch(p->graph, st));
+    // final renormalisation (GPU_Wigner4D.py:516-517)
+    return wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st);
+}
+
+extern "C" int wig4d_run(wig4d_plan* p, void* W, int iterations, double* d_history, void* stream) {
+    if (!p || !W || !d_history || iterations < 0) return WIG_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    return p->dtype == WIG_C128 ? run_impl<double2>(p, (double2*)W, iterations, d_history, st)
+                                : run_impl<float2>(p, (float2*)W, iterations, d_history, st);
+}
+
+extern "C" int wig4d_init_ho_ground(wig4d_plan* p, void* W, double x_mu, double y_mu, double px_mu,
+                                    double py_mu, double wx, double wy, double mass, void* stream) {
+    if (!p || !W) return WIG_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    if (p->dtype == WIG_C128)
+        k_init_ho<double2><<<grid_for(p->npts), 256, 0, st>>>((double2*)W, p->shape[0], p->shape[1], p->shape[2],
+                                                             p->shape[3], p->ob, x_mu, y_mu, px_mu, py_mu, wx, wy, mass);
+    else
+        k_init_ho<float2><<<grid_for(p->npts), 256, 0, st>>>((float2*)W, p->shape[0], p->shape[1], p->shape[2],
+                                                            p->shape[3], p->ob, x_mu, y_mu, px_mu, py_mu, wx, wy, mass);
+    WIG_LAUNCHED("k_init_ho");
+    return WIG_OK;
+}
+
+extern "C" int wig4d_init_gaussian(wig4d_plan* p, void* W, double mpy, double my, double mpx, double mx,
+                                   double spy, double sy, double spx, double sx, void* stream) {
+    if (!p || !W) return WIG_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    if (p->dtype == WIG_C128)
+        k_init_gauss<double2><<<grid_for(p->npts), 256, 0, st>>>((double2*)W, p->shape[0], p->shape[1], p->shape[2],
+                                                                p->shape[3], p->ob, mpy, my, mpx, mx, spy, sy, spx, sx);
+    else
+        k_init_gauss<float2><<<grid_for(p->npts), 256, 0, st>>>((float2*)W, p->shape[0], p->shape[1], p->shape[2],
+                                                               p->shape[3], p->ob, mpy, my, mpx, mx, spy, sy, spx, sx);
+    WIG_LAUNCHED("k_init_gauss");
+    return WIG_OK;
+}

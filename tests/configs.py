@@ -1,0 +1,65 @@
+"""Workloads of the parity tests and the bench: the W4D configurations.
+
+``config1`` is the 32^4 complex128 case (V = 0.5(x^2+y^2) + 0.1(x^4+y^4)
++ 0.05 x y, seeded Gaussian Wigner state, D = 0.01, dt = 0.01); ``config2``
+the 64^4 case with seeded quartic / coupling coefficients and a two-Gaussian
+cat state.  Ambiguity windows are chosen so that delta = 1/N on every axis
+(lambda_amp = pi/dx, theta_amp = pi/dp).
+"""
+import math
+
+import numpy as np
+
+
+def w4d_params(n, amp=8.0, q=0.1, kappa=0.05, D=0.01, dt=0.01, n_p=None):
+    n_p = n if n_p is None else n_p
+    dx = 2 * amp / n
+    dp = 2 * amp / n_p
+    return dict(
+        gridDIM_p_y=n_p, gridDIM_y=n, gridDIM_p_x=n_p, gridDIM_x=n,
+        p_y_amplitude=amp, y_amplitude=amp, p_x_amplitude=amp, x_amplitude=amp,
+        theta_y_amplitude=math.pi / dp, theta_x_amplitude=math.pi / dp,
+        lambda_y_amplitude=math.pi / dx, lambda_x_amplitude=math.pi / dx,
+        dt=dt, mass=1.0, timeSteps=0,
+        kineticString="0.5*(p_x*p_x + p_y*p_y)",
+        potentialString="0.5*(x*x + y*y) + %r*(pow(x,4) + pow(y,4)) + %r*x*y" % (q, kappa),
+        D_theta_x=D, D_theta_y=D, D_lambda_x=D, D_lambda_y=D)
+
+
+def centres(seed):
+    rng = np.random.default_rng(seed)
+    x0, y0 = rng.uniform(-2, 2, size=2)
+    px0, py0 = rng.uniform(-1, 1, size=2)
+    return float(x0), float(y0), float(px0), float(py0)
+
+
+def config1(seed=0, n=32):
+    return w4d_params(n, q=0.1, kappa=0.05, D=0.01, dt=0.01), centres(seed)
+
+
+def config2(seed=0, n=64):
+    rng = np.random.default_rng(seed + 1000)
+    q = float(rng.uniform(0.05, 0.2))
+    kappa = float(rng.uniform(0.0, 0.1))
+    return w4d_params(n, q=q, kappa=kappa, D=0.005, dt=0.005), centres(seed)
+
+
+def gaussian_xp(coords, c):
+    """(1/pi^2) exp(-sum (q - q0)^2) on the (x, p) grid; coords = (p_y, y, p_x, x)."""
+    x0, y0, px0, py0 = c
+    py, y, px, x = [np.asarray(v).reshape(s) for v, s in zip(
+        coords, [(-1, 1, 1, 1), (1, -1, 1, 1), (1, 1, -1, 1), (1, 1, 1, -1)])]
+    return (np.exp(-(x - x0) ** 2 - (px - px0) ** 2 - (y - y0) ** 2 - (py - py0) ** 2)
+            / np.pi ** 2).astype(np.complex128)
+
+
+def cat_xp(coords, c, sep=1.5):
+    """Two displaced Gaussians in superposition, as a Wigner function in (x, p):
+    W = G(q - a) + G(q + a) + 2 G(q) cos(2 (p . a_x - x . a_p)) (interference),
+    normalisation irrelevant (Run() renormalises)."""
+    x0, y0, px0, py0 = c
+    py, y, px, x = [np.asarray(v).reshape(s) for v, s in zip(
+        coords, [(-1, 1, 1, 1), (1, -1, 1, 1), (1, 1, -1, 1), (1, 1, 1, -1)])]
+    g = lambda dx, dy: np.exp(-(x - x0 - dx) ** 2 - (px - px0) ** 2 - (y - y0 - dy) ** 2 - (py - py0) ** 2)
+    w = g(sep, 0.0) + g(-sep, 0.0) + 2 * g(0.0, 0.0) * np.cos(2 * sep * (px - px0))
+    return (w / np.pi ** 2).astype(np.complex128)

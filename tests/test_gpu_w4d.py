@@ -1,0 +1,189 @@
+"""GPU parity of the scalar Wigner4D path against the NumPy oracle.
+
+Tolerances: complex128 (the drop-in) must match the oracle to 1e-12
+relative in norms and observables and 1e-10 in max|dW| / max|W|, the
+north-star bar; complex64 (the precision form) to 2e-5 relative per step
+budget over the short runs here.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from configs import config1, config2, w4d_params  # noqa: E402
+from frames import make_frame, rel_err  # noqa: E402
+from oracle.faft import faft  # noqa: E402
+from oracle.wigner4d import Wigner4DOracle  # noqa: E402
+from pywignercuda2_b200 import GPU_Wigner4D, GPUArray, _lib  # noqa: E402
+
+
+def _rand(shape, seed, dtype=np.complex128):
+    rng = np.random.default_rng(seed)
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("shape", [(16, 16, 32, 32), (32, 16, 16, 64), (16, 32, 16, 16)])
+@pytest.mark.parametrize("axis", [0, 1, 2, 3])
+@pytest.mark.parametrize("dn", [1.0, -1.0, 0.7, -0.83])
+def test_faft_kernel(dtype, shape, axis, dn):
+    a = _rand(shape, 3 + axis, dtype)
+    n = shape[axis]
+    d, delta = 0.37, dn / n
+    g = GPUArray.to_gpu(a)
+    sh = (ctypes.c_int * 4)(*shape)
+    wd = _lib.C128 if dtype == np.complex128 else _lib.C64
+    _lib.call("wig_faft", g.ptr, sh, wd, axis, d, delta, 0.5, None)
+    torch.cuda.synchronize()
+    want = 0.5 * faft(a.astype(np.complex128), axis, d, delta)
+    tol = 1e-13 if dtype == np.complex128 else 2e-6
+    assert rel_err(g.get(), want) < tol
+
+
+def test_faft_reference_shim_64():
+    a = _rand((64, 64, 64, 64), 9)
+    g = GPUArray.to_gpu(a)
+    _lib.call("FAFT64_4D_Z2Z", g.ptr, 0.25, 1.0 / 64, 0, 2, 1.0)
+    torch.cuda.synchronize()
+    assert rel_err(g.get(), faft(a, 2, 0.25, 1.0 / 64)) < 1e-13
+
+
+def _pair(params, dtype=np.complex128, **kw):
+    f = make_frame(GPU_Wigner4D, params, complex_dtype=dtype, **kw)
+    o = Wigner4DOracle(params)
+    return f, o
+
+
+@pytest.mark.parametrize("n", [16, 32])
+def test_init_kernels(n):
+    p, c = config1(0, n)
+    f, o = _pair(p)
+    f.HOscillatorGound_GPU(f.W_init_gpu, c[0], c[1], c[2], c[3], 1.0, 1.0, 1.0)
+    assert rel_err(f.W_init_gpu.get(), o.ho_ground(c[0], c[1], c[2], c[3], 1.0, 1.0, 1.0)) < 1e-15
+    f.Gaussian_GPU(f.W_init_gpu, 0.1, -0.2, 0.3, 0.4, 1.1, 0.9, 1.3, 0.7)
+    assert rel_err(f.W_init_gpu.get(), o.gaussian(0.1, -0.2, 0.3, 0.4, 1.1, 0.9, 1.3, 0.7)) < 1e-15
+
+
+@pytest.mark.parametrize("n", [16, 32, 64])
+def test_fused_halfsteps(n):
+    p, c = config1(1, n)
+    f, o = _pair(p)
+    W0 = o.ho_ground(c[0], c[1], c[2], c[3], 1.0, 1.0, 1.0) + 0.01 * _rand(f.shape, 5)
+    g = GPUArray.to_gpu(W0)
+    f.kinetic_halfstep(g)
+    want = o.x_to_lambda(o.x_to_lambda(W0) * o.kinetic_factor(), -1)
+    assert rel_err(g.get(), want) < 1e-12
+    g.set(W0)
+    f.potential_halfstep(g)
+    want = o.p_to_theta(o.p_to_theta(W0) * o.potential_factor(), -1)
+    assert rel_err(g.get(), want) < 1e-12
+
+
+def test_unfused_wrappers_and_phase_kernels():
+    p, c = config1(2, 16)
+    f, o = _pair(p)
+    W0 = _rand(f.shape, 11)
+    g = GPUArray.to_gpu(W0)
+    f.Fourier_X_To_Lambda_64_64_GPU(g)
+    f.exp_p_lambda_GPU(g)
+    f.Fourier_Lambda_To_X_64_64_GPU(g)
+    f.Fourier_P_To_Theta_64_64_GPU(g)
+    f.exp_x_theta_GPU(g)
+    f.Fourier_Theta_To_P_64_64_GPU(g)
+    want = o.x_to_lambda(o.x_to_lambda(W0) * o.kinetic_factor(), -1)
+    want = o.p_to_theta(o.p_to_theta(want) * o.potential_factor(), -1)
+    assert rel_err(g.get(), want) < 1e-12
+
+
+def test_reductions():
+    p, c = config1(3, 32)
+    f, o = _pair(p)
+    W0 = o.ho_ground(c[0], c[1], c[2], c[3], 1.0, 1.0, 1.0) * (1.0 + 0.3j)
+    g = GPUArray.to_gpu(W0)
+    assert abs(f.Norm_GPU(g) - o.norm(W0)) < 1e-13 * abs(o.norm(W0))
+    ob = o.observables(W0)
+    for name in ["average_x", "average_p_x", "average_x_square", "average_p_x_square", "average_y",
+                 "average_p_y", "average_y_square", "average_p_y_square"]:
+        got = getattr(f, name.replace("average", "Average") + "_GPU")(g).get()
+        assert abs(got - ob[name]) <= 1e-12 * max(1.0, abs(ob[name])), name
+    assert abs(f.Energy_GPU(g).get() - ob["energy"]) <= 1e-12 * abs(ob["energy"])
+
+
+def _run_both(params, init, iters, dtype=np.complex128):
+    f, o = _pair(params, dtype)
+    W0 = init(f, o)
+    f.W_init_gpu.set(W0.astype(dtype))
+    f.timeSteps = iters - 1
+    f.fileName = None
+    f.Run()
+    Wo, obs = o.run(W0.astype(np.complex64).astype(np.complex128) if dtype == np.complex64 else W0, iters - 1)
+    return f, Wo, obs
+
+
+OBS = ["average_x", "average_p_x", "average_x_square", "average_p_x_square", "average_y",
+       "average_p_y", "average_y_square", "average_p_y_square", "energy"]
+
+
+@pytest.mark.parametrize("n", [16, 32])
+def test_run_config1_parity(n):
+    p, c = config1(0, n)
+    init = lambda f, o: o.ho_ground(c[0], c[1], c[2], c[3], 1.0, 1.0, 1.0) / np.pi ** 2
+    f, Wo, obs = _run_both(p, init, 21)
+    for name in OBS:
+        assert rel_err(getattr(f, name), obs[name]) < 1e-12, name
+    assert rel_err(f.norm, obs["norms"]) < 1e-12
+    assert rel_err(f.W_init_gpu.get(), Wo) < 1e-10
+
+
+def test_run_general_delta_unfused():
+    """Notebook-style windows (delta N != 1) take the dense unfused path."""
+    p = w4d_params(16, D=0.01, dt=0.01)
+    p.update(theta_x_amplitude=9.0, theta_y_amplitude=9.0, lambda_x_amplitude=9.0, lambda_y_amplitude=9.0)
+    init = lambda f, o: o.ho_ground(0.5, -0.5, 1.0, 1.0, 1.0, 1.0, 1.0)
+    f, Wo, obs = _run_both(p, init, 6)
+    for name in OBS:
+        assert rel_err(getattr(f, name), obs[name]) < 1e-12, name
+    assert rel_err(f.W_init_gpu.get(), Wo) < 1e-10
+
+
+def test_run_precision_form_c64():
+    p, c = config1(4, 32)
+    init = lambda f, o: o.ho_ground(c[0], c[1], c[2], c[3], 1.0, 1.0, 1.0)
+    f, Wo, obs = _run_both(p, init, 21, np.complex64)
+    for name in OBS:
+        assert rel_err(getattr(f, name), obs[name]) < 2e-5, name
+    assert rel_err(f.W_init_gpu.get(), Wo) < 2e-4
+
+
+def test_run_cat_state_config2_prefix():
+    from configs import cat_xp
+    p, c = config2(0, 32)
+    f, o = _pair(p)
+    W0 = cat_xp(f._coords, c)
+    f.W_init_gpu.set(W0)
+    f.timeSteps = 9
+    f.fileName = None
+    f.Run()
+    Wo, obs = o.run(W0, 9)
+    assert (W0.real < 0).any()
+    for name in OBS:
+        assert rel_err(getattr(f, name), obs[name]) < 1e-12, name
+    assert rel_err(f.W_init_gpu.get(), Wo) < 1e-10
+
+
+def test_nonfinite_state_raises():
+    p, c = config1(0, 16)
+    f, o = _pair(p)
+    W0 = o.ho_ground(c[0], c[1], c[2], c[3], 1.0, 1.0, 1.0)
+    W0[3, 3, 3, 3] = np.nan
+    f.W_init_gpu.set(W0)
+    f.timeSteps = 1
+    f.fileName = None
+    with pytest.raises(FloatingPointError):
+        f.Run()
