@@ -46,11 +46,13 @@ def _clock_sampler(local):
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
     try:
-        return subprocess.Popen(["nvidia-smi", "-i", str(local), "--query-gpu=" + q,
-                                 "--format=csv,noheader,nounits", "-lms", "200"],
-                                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        p = subprocess.Popen(["nvidia-smi", "-i", str(local), "--query-gpu=" + q,
+                              "--format=csv,noheader,nounits", "-lms", "100"],
+                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
     except OSError:
         return None
+    time.sleep(1.0)   # nvidia-smi needs a moment before its first sample
+    return p
 
 
 def _clock_summary(proc):
@@ -68,7 +70,7 @@ def _clock_summary(proc):
     sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
     mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
     names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-    reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]})
+    reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
     return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
             "reasons": reasons, "samples": len(rows)}
 
@@ -145,7 +147,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -27,6 +27,7 @@
 
 #include "common.cuh"
 #include "fft_smem.cuh"
+#include "lanes64.cuh"
 
 void* wig_dense_matrix(int n, double delta, int dtype, cudaStream_t st);
 
@@ -97,15 +98,38 @@ __device__ __forceinline__ void block_sum_partials(double (&a)[NPART], double* s
 }
 
 // ---------------------------------------------------------------------------
+// Plane layout in shared memory: rows of the plane are padded by one element
+// (row stride NX + 1) so that a warp walking down a column, or across the
+// rows at a fixed column, touches every bank once; every FFT pass then maps
+// consecutive threads to consecutive lines (LINE_FAST) and is conflict-free.
+// Loads and stores issue all of a thread's global accesses before touching
+// shared memory, so each thread keeps PER requests in flight.
+// ---------------------------------------------------------------------------
+template <int NY, int NX, int NT>
+struct PlaneCfg {
+    static constexpr int LD = NX + 1;                 // padded row stride
+    static constexpr int PTS = NY * NX;
+    static constexpr int PER = (PTS + NT - 1) / NT;   // points per thread
+    // two CTAs per SM (64 registers) while a thread holds at most 8 points
+    static constexpr int MINB = (NT >= 512 && PER <= 8) ? 2 : 1;
+};
+
+template <class C, int NY, int NX>
+static constexpr size_t plane_bytes() {
+    return sizeof(C) * ((size_t)NY * (NX + 1) + NX + NY);
+}
+
+// ---------------------------------------------------------------------------
 // Fused kinetic half-step: CTA = one (p_y, p_x) plane of NY x NX points.
 // ---------------------------------------------------------------------------
 template <class C, int NY, int NX, int NT>
-__global__ void __launch_bounds__(NT) k_kinetic(C* __restrict__ W, int npy, int npx,
+__global__ void __launch_bounds__(NT, PlaneCfg<NY, NX, NT>::MINB) k_kinetic(C* __restrict__ W, int npy, int npx,
                                                 FactorSet<C> F, double2 scale,
                                                 const double* __restrict__ d_norm) {
+    typedef PlaneCfg<NY, NX, NT> P;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* s = reinterpret_cast<C*>(smraw);
-    C* twx = s + NY * NX;
+    C* twx = s + NY * P::LD;
     C* twy = twx + NX;
     const int ipx = blockIdx.x % npx, ipy = blockIdx.x / npx;
     make_twiddles(twx, NX);
@@ -114,37 +138,51 @@ __global__ void __launch_bounds__(NT) k_kinetic(C* __restrict__ W, int npy, int 
 
     const long long rowstride = (long long)npx * NX;
     C* g = W + ((long long)ipy * NY * npx + ipx) * NX;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < NY * NX; e += NT) {
-        const int y = e / NX, x = e % NX;
-        C v = g[y * rowstride + x];
-        if ((x + y) & 1) v = cneg(v);
-        s[e] = v;
+    {
+        C v[P::PER];
+#pragma unroll
+        for (int i = 0; i < P::PER; ++i) {
+            const int e = threadIdx.x + i * NT;
+            if (P::PTS % NT == 0 || e < P::PTS) v[i] = g[(e / NX) * rowstride + (e % NX)];
+        }
+#pragma unroll
+        for (int i = 0; i < P::PER; ++i) {
+            const int e = threadIdx.x + i * NT;
+            if (P::PTS % NT == 0 || e < P::PTS) {
+                const int y = e / NX, x = e % NX;
+                s[y * P::LD + x] = ((x + y) & 1) ? cneg(v[i]) : v[i];
+            }
+        }
     }
     __syncthreads();
-    LineMap rows{1, NX, 0, 1}, cols{1, 1, 0, NX};
-    fft_lines<C, NX, NY, NT, true, false>(s, rows, twx);
+    const LineMap rows{1, P::LD, 0, 1}, cols{1, 1, 0, P::LD};
+    fft_lines<C, NX, NY, NT, true, true>(s, rows, twx);
     fft_lines<C, NY, NX, NT, true, true>(s, cols, ty);
 
     double2 c0 = scale;
     if (d_norm) c0 = zmul(c0, zinv(make_double2(d_norm[0], d_norm[1])));
     const C cc = to_c<C>(c0);
     const long long lin0 = ((long long)ipy * NY * npx + ipx) * NX;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < NY * NX; e += NT) {
-        const int y = e / NX, x = e % NX;
-        C f = factor_at(F, ipy, y, ipx, x, lin0 + y * rowstride + x, cc);
-        s[e] = cmul(s[e], f);
+#pragma unroll
+    for (int i = 0; i < P::PER; ++i) {
+        const int e = threadIdx.x + i * NT;
+        if (P::PTS % NT == 0 || e < P::PTS) {
+            const int y = e / NX, x = e % NX;
+            C f = factor_at(F, ipy, y, ipx, x, lin0 + y * rowstride + x, cc);
+            s[y * P::LD + x] = cmul(s[y * P::LD + x], f);
+        }
     }
     __syncthreads();
     fft_lines<C, NY, NX, NT, false, true>(s, cols, ty);
-    fft_lines<C, NX, NY, NT, false, false>(s, rows, twx);
-#pragma unroll 4
-    for (int e = threadIdx.x; e < NY * NX; e += NT) {
-        const int y = e / NX, x = e % NX;
-        C v = s[e];
-        if ((x + y) & 1) v = cneg(v);
-        g[y * rowstride + x] = v;
+    fft_lines<C, NX, NY, NT, false, true>(s, rows, twx);
+#pragma unroll
+    for (int i = 0; i < P::PER; ++i) {
+        const int e = threadIdx.x + i * NT;
+        if (P::PTS % NT == 0 || e < P::PTS) {
+            const int y = e / NX, x = e % NX;
+            C v = s[y * P::LD + x];
+            g[y * rowstride + x] = ((x + y) & 1) ? cneg(v) : v;
+        }
     }
 }
 
@@ -153,12 +191,13 @@ __global__ void __launch_bounds__(NT) k_kinetic(C* __restrict__ W, int npy, int 
 // Epilogue: partial sums of the next iteration's reductions.
 // ---------------------------------------------------------------------------
 template <class C, int NPY, int NPX, int NT>
-__global__ void __launch_bounds__(NT) k_potential(C* __restrict__ W, int ny, int nx,
+__global__ void __launch_bounds__(NT, PlaneCfg<NPY, NPX, NT>::MINB) k_potential(C* __restrict__ W, int ny, int nx,
                                                   FactorSet<C> F, double2 scale, ObsTabs ob,
                                                   double* __restrict__ partials) {
+    typedef PlaneCfg<NPY, NPX, NT> P;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* s = reinterpret_cast<C*>(smraw);
-    C* twx = s + NPY * NPX;
+    C* twx = s + NPY * P::LD;
     C* twy = twx + NPX;
     const int ix = blockIdx.x % nx, iy = blockIdx.x / nx;
     make_twiddles(twx, NPX);
@@ -168,53 +207,507 @@ __global__ void __launch_bounds__(NT) k_potential(C* __restrict__ W, int ny, int
     const long long pxs = nx;                       // stride of p_x
     const long long pys = (long long)ny * NPX * nx; // stride of p_y
     C* g = W + (long long)iy * NPX * nx + ix;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < NPY * NPX; e += NT) {
-        const int py = e / NPX, px = e % NPX;
-        C v = g[py * pys + px * pxs];
-        if ((px + py) & 1) v = cneg(v);
-        s[e] = v;
+    {
+        C v[P::PER];
+#pragma unroll
+        for (int i = 0; i < P::PER; ++i) {
+            const int e = threadIdx.x + i * NT;
+            if (P::PTS % NT == 0 || e < P::PTS) v[i] = g[(e / NPX) * pys + (e % NPX) * pxs];
+        }
+#pragma unroll
+        for (int i = 0; i < P::PER; ++i) {
+            const int e = threadIdx.x + i * NT;
+            if (P::PTS % NT == 0 || e < P::PTS) {
+                const int py = e / NPX, px = e % NPX;
+                s[py * P::LD + px] = ((px + py) & 1) ? cneg(v[i]) : v[i];
+            }
+        }
     }
     __syncthreads();
-    LineMap rows{1, NPX, 0, 1}, cols{1, 1, 0, NPX};
-    fft_lines<C, NPX, NPY, NT, true, false>(s, rows, twx);
+    const LineMap rows{1, P::LD, 0, 1}, cols{1, 1, 0, P::LD};
+    fft_lines<C, NPX, NPY, NT, true, true>(s, rows, twx);
     fft_lines<C, NPY, NPX, NT, true, true>(s, cols, ty);
     const C cc = to_c<C>(scale);
     const long long lin0 = (long long)iy * NPX * nx + ix;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < NPY * NPX; e += NT) {
-        const int py = e / NPX, px = e % NPX;
-        C f = factor_at(F, py, iy, px, ix, lin0 + py * pys + px * pxs, cc);
-        s[e] = cmul(s[e], f);
+#pragma unroll
+    for (int i = 0; i < P::PER; ++i) {
+        const int e = threadIdx.x + i * NT;
+        if (P::PTS % NT == 0 || e < P::PTS) {
+            const int py = e / NPX, px = e % NPX;
+            C f = factor_at(F, py, iy, px, ix, lin0 + py * pys + px * pxs, cc);
+            s[py * P::LD + px] = cmul(s[py * P::LD + px], f);
+        }
     }
     __syncthreads();
     fft_lines<C, NPY, NPX, NT, false, true>(s, cols, ty);
-    fft_lines<C, NPX, NPY, NT, false, false>(s, rows, twx);
+    fft_lines<C, NPX, NPY, NT, false, true>(s, rows, twx);
 
     double a[NPART];
 #pragma unroll
     for (int i = 0; i < NPART; ++i) a[i] = 0.0;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < NPY * NPX; e += NT) {
-        const int py = e / NPX, px = e % NPX;
-        C v = s[e];
-        if ((px + py) & 1) v = cneg(v);
-        g[py * pys + px * pxs] = v;
-        if (partials) {
-            const double2 w = to_d2(v);
-            const double qx = __ldg(ob.cpx + px), qy = __ldg(ob.cpy + py);
-            const double k = __ldg(ob.ep + py * NPX + px);
-            a[0] += w.x; a[1] += w.y;
-            a[2] = fma(qx, w.x, a[2]); a[3] = fma(qx, w.y, a[3]);
-            a[4] = fma(qx * qx, w.x, a[4]); a[5] = fma(qx * qx, w.y, a[5]);
-            a[6] = fma(qy, w.x, a[6]); a[7] = fma(qy, w.y, a[7]);
-            a[8] = fma(qy * qy, w.x, a[8]); a[9] = fma(qy * qy, w.y, a[9]);
-            a[10] = fma(k, w.x, a[10]); a[11] = fma(k, w.y, a[11]);
+#pragma unroll
+    for (int i = 0; i < P::PER; ++i) {
+        const int e = threadIdx.x + i * NT;
+        if (P::PTS % NT == 0 || e < P::PTS) {
+            const int py = e / NPX, px = e % NPX;
+            C v = s[py * P::LD + px];
+            if ((px + py) & 1) v = cneg(v);
+            g[py * pys + px * pxs] = v;
+            if (partials) {
+                const double2 w = to_d2(v);
+                const double qx = __ldg(ob.cpx + px), qy = __ldg(ob.cpy + py);
+                const double k = __ldg(ob.ep + py * NPX + px);
+                a[0] += w.x; a[1] += w.y;
+                a[2] = fma(qx, w.x, a[2]); a[3] = fma(qx, w.y, a[3]);
+                a[4] = fma(qx * qx, w.x, a[4]); a[5] = fma(qx * qx, w.y, a[5]);
+                a[6] = fma(qy, w.x, a[6]); a[7] = fma(qy, w.y, a[7]);
+                a[8] = fma(qy * qy, w.x, a[8]); a[9] = fma(qy * qy, w.y, a[9]);
+                a[10] = fma(k, w.x, a[10]); a[11] = fma(k, w.y, a[11]);
+            }
         }
     }
     if (partials) {
         __syncthreads();   // smem reused for the block reduction
         block_sum_partials<NT>(a, reinterpret_cast<double*>(smraw), partials + (long long)blockIdx.x * NPART);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Run() kernels for 64 x 64 x 64 x 64 grids: register-resident transforms
+// (lanes64.cuh) and a ping-pong layout between the two half-steps.
+//
+//   k_kin64: reads W in the reference layout L0 = [p_y][y][p_x][x] (each
+//            (y, x) plane is 64 rows of 1 KB), writes T in the transposed
+//            layout L1 = [y][x][p_y][p_x];
+//   k_pot64: reads T (each (p_y, p_x) plane is one contiguous 64 KB block),
+//            writes W in L0 and the partial sums of the observables.
+// Every global load is a contiguous 128-byte run per 8 lanes; the stores
+// are 16-byte (8-byte) scatters whose sectors are completed in L2 by the
+// CTAs of the neighbouring planes, which run at the same time.
+// ---------------------------------------------------------------------------
+template <class C>
+__global__ void __launch_bounds__(lanes64::NT, 2) k_kin64(const C* __restrict__ W, C* __restrict__ T,
+                                                          int npy, int npx, FactorSet<C> F, double2 scale,
+                                                          const double* __restrict__ d_norm) {
+    using namespace lanes64;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* s = reinterpret_cast<C*>(smraw);
+    C* tw = s + 64 * LD;
+    const int tid = threadIdx.x, grp = tid >> 3, q = tid & 7, gi = grp & 3;
+    C* ws = s + (tid >> 5) * 4 * LD;
+    const int ipx = blockIdx.x % npx, ipy = blockIdx.x / npx;
+    make_twiddles(tw, 64);
+    const C* src = W + (((long long)ipy * 64 + grp) * npx + ipx) * 64;
+    C v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const C t = src[q + 8 * r];
+        v[r] = ((grp + q) & 1) ? cneg(t) : t;   // x = q + 8 r: parity of x + y is that of q + grp
+    }
+    double2 c0 = scale;
+    if (d_norm) c0 = zmul(c0, zinv(make_double2(d_norm[0], d_norm[1])));
+    const C cc = to_c<C>(c0);
+    __syncthreads();
+    fft64<C, true>(v, ws, gi, q, tw);                 // along x: v[k2] = (y = grp, kx = q + 8 k2)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s[grp * LD + q + 8 * k] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = s[(q + 8 * r) * LD + grp];
+    __syncthreads();
+    fft64<C, true>(v, ws, gi, q, tw);                 // along y: v[k2] = (ky = q + 8 k2, kx = grp)
+    const long long lin0 = ((long long)ipy * 64 * npx + ipx) * 64 + grp;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int ky = q + 8 * k;
+        v[k] = cmul(v[k], factor_at(F, ipy, ky, ipx, grp, lin0 + (long long)ky * npx * 64, cc));
+    }
+    fft64<C, false>(v, ws, gi, q, tw);                // v[k2] = (y = q + 8 k2, kx = grp)
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s[(q + 8 * k) * LD + grp] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = s[grp * LD + q + 8 * r];
+    __syncthreads();
+    fft64<C, false>(v, ws, gi, q, tw);                // v[k2] = (y = grp, x = q + 8 k2)
+    C* dst = T + ((long long)grp * 64 * npy + ipy) * npx + ipx;
+    const long long xs = (long long)npy * npx;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int x = q + 8 * k;
+        dst[x * xs] = ((grp + x) & 1) ? cneg(v[k]) : v[k];
+    }
+}
+
+template <class C>
+__global__ void __launch_bounds__(lanes64::NT, 2) k_pot64(const C* __restrict__ T, C* __restrict__ W,
+                                                          int ny, int nx, FactorSet<C> F, double2 scale,
+                                                          ObsTabs ob, double* __restrict__ partials) {
+    using namespace lanes64;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* s = reinterpret_cast<C*>(smraw);
+    C* tw = s + 64 * LD;
+    const int tid = threadIdx.x, grp = tid >> 3, q = tid & 7, gi = grp & 3;
+    C* ws = s + (tid >> 5) * 4 * LD;
+    const int ix = blockIdx.x % nx, iy = blockIdx.x / nx;
+    make_twiddles(tw, 64);
+    const C* src = T + ((long long)blockIdx.x * 64 + grp) * 64;   // row p_y = grp
+    C v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const C t = src[q + 8 * r];
+        v[r] = ((grp + q) & 1) ? cneg(t) : t;   // x = q + 8 r: parity of x + y is that of q + grp
+    }
+    const C cc = to_c<C>(scale);
+    __syncthreads();
+    fft64<C, true>(v, ws, gi, q, tw);                 // along p_x
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s[grp * LD + q + 8 * k] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = s[(q + 8 * r) * LD + grp];
+    __syncthreads();
+    fft64<C, true>(v, ws, gi, q, tw);                 // along p_y: (theta_y = q + 8 k2, theta_x = grp)
+    const long long pys = (long long)ny * 64 * nx;
+    const long long lin0 = ((long long)iy * 64 + grp) * nx + ix;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int ky = q + 8 * k;
+        v[k] = cmul(v[k], factor_at(F, ky, iy, grp, ix, lin0 + ky * pys, cc));
+    }
+    fft64<C, false>(v, ws, gi, q, tw);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s[(q + 8 * k) * LD + grp] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = s[grp * LD + q + 8 * r];
+    __syncthreads();
+    fft64<C, false>(v, ws, gi, q, tw);                // (p_y = grp, p_x = q + 8 k2)
+    C* dst = W + (long long)grp * pys + (long long)iy * 64 * nx + ix;
+    double a[NPART];
+#pragma unroll
+    for (int i = 0; i < NPART; ++i) a[i] = 0.0;
+    const double qy = __ldg(ob.cpy + grp);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int px = q + 8 * k;
+        const C val = ((grp + px) & 1) ? cneg(v[k]) : v[k];
+        dst[(long long)px * nx] = val;
+        const double2 w = to_d2(val);
+        const double qx = __ldg(ob.cpx + px), kk = __ldg(ob.ep + grp * 64 + px);
+        a[0] += w.x; a[1] += w.y;
+        a[2] = fma(qx, w.x, a[2]); a[3] = fma(qx, w.y, a[3]);
+        a[4] = fma(qx * qx, w.x, a[4]); a[5] = fma(qx * qx, w.y, a[5]);
+        a[6] = fma(qy, w.x, a[6]); a[7] = fma(qy, w.y, a[7]);
+        a[8] = fma(qy * qy, w.x, a[8]); a[9] = fma(qy * qy, w.y, a[9]);
+        a[10] = fma(kk, w.x, a[10]); a[11] = fma(kk, w.y, a[11]);
+    }
+    __syncthreads();
+    block_sum_partials<NT>(a, reinterpret_cast<double*>(smraw), partials + (long long)blockIdx.x * NPART);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent versions (one CTA of 512 threads per SM, looping over planes).
+//
+// * The next plane's global loads are issued into registers before the
+//   current plane is transformed, so they are in flight during the compute.
+// * No centring sign flips: with S = (-1)^(x+y), S IFFT2(F FFT2(S w)) equals
+//   IFFT2(F' FFT2(w)) where F'[k] = F[k + N/2] (indices mod N), so the factor
+//   is simply read at frequencies shifted by N/2.
+// * The factor of a plane is the product of per-plane vectors along each
+//   in-plane axis (built once per plane in shared memory from the pairwise
+//   tables) times, only if present, tables over both in-plane axes.
+// * k_pot64p accumulates every observable sum (11 complex) per thread over
+//   all of its planes; one partial row per CTA.
+// ---------------------------------------------------------------------------
+#define NSUM 22   // sum W, xW, x^2 W, p_x W, p_x^2 W, yW, y^2 W, p_y W, p_y^2 W, K W, V W (complex)
+
+template <class C>
+struct PlaneFactors {
+    // in-plane axes (ay: the row index axis, ax: the column index axis) and
+    // the two fixed axes of the CTA's plane
+    int ay, ax;
+};
+
+// Build fy[0..63] (factor along the row-frequency axis, c0 folded in) and
+// fx[0..63] for the plane with fixed indices (fixed0 on axis f0, fixed1 on f1).
+// Tables over both in-plane axes or full 4-D tables set *per_point.
+template <class C>
+__device__ __forceinline__ void build_plane_factors(const FactorSet<C>& F, int ay, int ax, int f0, int i_f0,
+                                                    int f1, int i_f1, double2 c0, double2* fy, double2* fx) {
+    const int t = threadIdx.x;
+    if (t < 128) {
+        const bool along_y = t < 64;
+        const int k = t & 63;
+        const int kk = (k + 32) & 63;          // N/2-shifted frequency (see above)
+        const int axis = along_y ? ay : ax;
+        double2 acc = along_y ? c0 : make_double2(1.0, 0.0);
+        for (int j = 0; j < F.n; ++j) {
+            const int a = F.ia[j], b = F.ib[j];
+            if (a < 0) continue;                                  // full table: per point
+            const bool ina = (a == ay || a == ax), inb = (b >= 0) && (b == ay || b == ax);
+            if (ina && inb) continue;                             // both in-plane: per point
+            // scalar tables (no in-plane axis) go into fy only
+            const bool touches = (a == axis) || (b == axis);
+            const bool scalar = !ina && !inb;
+            if (!(touches || (scalar && along_y))) continue;
+            auto idx_of = [&](int ax_) { return ax_ == axis ? kk : (ax_ == f0 ? i_f0 : i_f1); };
+            long long idx = (b < 0) ? idx_of(a) : (long long)idx_of(a) * F.nb[j] + idx_of(b);
+            acc = zmul(acc, to_d2(F.data[j][idx]));
+        }
+        (along_y ? fy : fx)[k] = acc;
+    }
+}
+
+template <class C>
+__device__ __forceinline__ bool has_per_point(const FactorSet<C>& F, int ay, int ax) {
+    for (int j = 0; j < F.n; ++j) {
+        const int a = F.ia[j], b = F.ib[j];
+        if (a < 0) return true;
+        if ((a == ay || a == ax) && b >= 0 && (b == ay || b == ax)) return true;
+    }
+    return false;
+}
+
+// per-point part (only tables over both in-plane axes or full tables)
+template <class C>
+__device__ __forceinline__ C per_point_factor(const FactorSet<C>& F, int ay, int ax, int i0, int i1, int i2,
+                                              int i3, long long lin, C acc) {
+    for (int j = 0; j < F.n; ++j) {
+        const int a = F.ia[j], b = F.ib[j];
+        long long idx;
+        if (a < 0) idx = lin;
+        else if ((a == ay || a == ax) && b >= 0 && (b == ay || b == ax))
+            idx = (long long)sel4(a, i0, i1, i2, i3) * F.nb[j] + sel4(b, i0, i1, i2, i3);
+        else continue;
+        acc = cmul(acc, __ldg(F.data[j] + idx));
+    }
+    return acc;
+}
+
+template <class C>
+__global__ void __launch_bounds__(lanes64::NT, 1) k_kin64p(const C* __restrict__ W, C* __restrict__ T,
+                                                           int npy, int npx, FactorSet<C> F, double2 scale,
+                                                           const double* __restrict__ d_norm) {
+    using namespace lanes64;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* s = reinterpret_cast<C*>(smraw);
+    C* tw = s + 64 * LD;
+    double2* fy = reinterpret_cast<double2*>(tw + 64);
+    double2* fx = fy + 64;
+    const int tid = threadIdx.x, grp = tid >> 3, q = tid & 7, gi = grp & 3;
+    C* ws = s + (tid >> 5) * 4 * LD;
+    const int nplanes = npy * npx;
+    make_twiddles(tw, 64);
+    double2 c0 = scale;
+    if (d_norm) c0 = zmul(c0, zinv(make_double2(d_norm[0], d_norm[1])));
+    const bool pp = has_per_point(F, 1, 3);
+    const long long rs = (long long)npx * 64;   // stride of y in W
+    int plane = blockIdx.x;
+    C nv[8];
+    if (plane < nplanes) {
+        const C* src = W + (((long long)(plane / npx) * 64 + grp) * npx + plane % npx) * 64;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) nv[r] = src[q + 8 * r];
+    }
+    for (; plane < nplanes; plane += gridDim.x) {
+        C v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = nv[r];
+        const int next = plane + gridDim.x;
+        if (next < nplanes) {
+            const C* src = W + (((long long)(next / npx) * 64 + grp) * npx + next % npx) * 64;
+#pragma unroll
+            for (int r = 0; r < 8; ++r) nv[r] = src[q + 8 * r];
+        }
+        const int ipx = plane % npx, ipy = plane / npx;
+        build_plane_factors(F, 1, 3, 0, ipy, 2, ipx, c0, fy, fx);
+        __syncthreads();                                  // twiddles, factors; previous plane done
+        fft64<C, true>(v, ws, gi, q, tw);                 // along x: (y = grp, kx = q + 8 k)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s[grp * LD + q + 8 * k] = v[k];
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = s[(q + 8 * r) * LD + grp];
+        __syncthreads();
+        fft64<C, true>(v, ws, gi, q, tw);                 // along y: (ky = q + 8 k, kx = grp)
+        const C fxv = to_c<C>(fx[grp]);
+        const int kxs = (grp + 32) & 63;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            C f = cmul(to_c<C>(fy[q + 8 * k]), fxv);
+            if (pp) {
+                const int kys = (q + 8 * k + 32) & 63;
+                f = per_point_factor(F, 1, 3, ipy, kys, ipx, kxs,
+                                     (((long long)ipy * 64 + kys) * npx + ipx) * 64 + kxs, f);
+            }
+            v[k] = cmul(v[k], f);
+        }
+        fft64<C, false>(v, ws, gi, q, tw);                // (y = q + 8 k, kx = grp)
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s[(q + 8 * k) * LD + grp] = v[k];
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = s[grp * LD + q + 8 * r];
+        __syncthreads();
+        fft64<C, false>(v, ws, gi, q, tw);                // (y = grp, x = q + 8 k)
+        C* dst = T + ((long long)grp * 64 * npy + ipy) * npx + ipx;
+        const long long xs = (long long)npy * npx;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) dst[(q + 8 * k) * xs] = v[k];
+        (void)rs;
+    }
+}
+
+template <class C>
+__global__ void __launch_bounds__(lanes64::NT, 1) k_pot64p(const C* __restrict__ T, C* __restrict__ W,
+                                                           int ny, int nx, FactorSet<C> F, double2 scale,
+                                                           ObsTabs ob, double* __restrict__ partials) {
+    using namespace lanes64;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* s = reinterpret_cast<C*>(smraw);
+    C* tw = s + 64 * LD;
+    double2* fy = reinterpret_cast<double2*>(tw + 64);
+    double2* fx = fy + 64;
+    const int tid = threadIdx.x, grp = tid >> 3, q = tid & 7, gi = grp & 3;
+    C* ws = s + (tid >> 5) * 4 * LD;
+    const int nplanes = ny * nx;
+    make_twiddles(tw, 64);
+    const bool pp = has_per_point(F, 0, 2);
+    const long long pys = (long long)ny * 64 * nx;
+    double a[NSUM];
+#pragma unroll
+    for (int i = 0; i < NSUM; ++i) a[i] = 0.0;
+    const double qy = __ldg(ob.cpy + grp);
+    int plane = blockIdx.x;
+    C nv[8];
+    if (plane < nplanes) {
+        const C* src = T + ((long long)plane * 64 + grp) * 64;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) nv[r] = src[q + 8 * r];
+    }
+    for (; plane < nplanes; plane += gridDim.x) {
+        C v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = nv[r];
+        const int next = plane + gridDim.x;
+        if (next < nplanes) {
+            const C* src = T + ((long long)next * 64 + grp) * 64;
+#pragma unroll
+            for (int r = 0; r < 8; ++r) nv[r] = src[q + 8 * r];
+        }
+        const int ix = plane % nx, iy = plane / nx;
+        build_plane_factors(F, 0, 2, 1, iy, 3, ix, scale, fy, fx);
+        __syncthreads();
+        fft64<C, true>(v, ws, gi, q, tw);                 // along p_x
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s[grp * LD + q + 8 * k] = v[k];
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = s[(q + 8 * r) * LD + grp];
+        __syncthreads();
+        fft64<C, true>(v, ws, gi, q, tw);                 // along p_y: (theta_y = q + 8 k, theta_x = grp)
+        const C fxv = to_c<C>(fx[grp]);
+        const int kxs = (grp + 32) & 63;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            C f = cmul(to_c<C>(fy[q + 8 * k]), fxv);
+            if (pp) {
+                const int kys = (q + 8 * k + 32) & 63;
+                f = per_point_factor(F, 0, 2, kys, iy, kxs, ix,
+                                     (((long long)kys * ny + iy) * 64 + kxs) * nx + ix, f);
+            }
+            v[k] = cmul(v[k], f);
+        }
+        fft64<C, false>(v, ws, gi, q, tw);
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s[(q + 8 * k) * LD + grp] = v[k];
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = s[grp * LD + q + 8 * r];
+        __syncthreads();
+        fft64<C, false>(v, ws, gi, q, tw);                // (p_y = grp, p_x = q + 8 k)
+        C* dst = W + (long long)grp * pys + (long long)iy * 64 * nx + ix;
+        double sw0 = 0.0, sw1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int px = q + 8 * k;
+            dst[(long long)px * nx] = v[k];
+            const double2 w = to_d2(v[k]);
+            const double qx = __ldg(ob.cpx + px), kk = __ldg(ob.ep + grp * 64 + px);
+            sw0 += w.x; sw1 += w.y;
+            a[6] = fma(qx, w.x, a[6]); a[7] = fma(qx, w.y, a[7]);
+            a[8] = fma(qx * qx, w.x, a[8]); a[9] = fma(qx * qx, w.y, a[9]);
+            a[18] = fma(kk, w.x, a[18]); a[19] = fma(kk, w.y, a[19]);
+        }
+        const double x = __ldg(ob.cx + ix), y = __ldg(ob.cy + iy), V = __ldg(ob.ex + iy * nx + ix);
+        a[0] += sw0; a[1] += sw1;
+        a[2] = fma(x, sw0, a[2]); a[3] = fma(x, sw1, a[3]);
+        a[4] = fma(x * x, sw0, a[4]); a[5] = fma(x * x, sw1, a[5]);
+        a[10] = fma(y, sw0, a[10]); a[11] = fma(y, sw1, a[11]);
+        a[12] = fma(y * y, sw0, a[12]); a[13] = fma(y * y, sw1, a[13]);
+        a[14] = fma(qy, sw0, a[14]); a[15] = fma(qy, sw1, a[15]);
+        a[16] = fma(qy * qy, sw0, a[16]); a[17] = fma(qy * qy, sw1, a[17]);
+        a[20] = fma(V, sw0, a[20]); a[21] = fma(V, sw1, a[21]);
+    }
+    // block reduction of NSUM doubles (fixed order)
+#pragma unroll
+    for (int i = 0; i < NSUM; ++i) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a[i] += __shfl_down_sync(0xffffffffu, a[i], o);
+    }
+    __syncthreads();
+    double* sm = reinterpret_cast<double*>(smraw);
+    const int w = tid >> 5, l = tid & 31;
+    if (l == 0) {
+#pragma unroll
+        for (int i = 0; i < NSUM; ++i) sm[w * NSUM + i] = a[i];
+    }
+    __syncthreads();
+    if (tid < NSUM) {
+        double t = 0.0;
+        for (int k = 0; k < NT / 32; ++k) t += sm[k * NSUM + tid];
+        partials[(long long)blockIdx.x * NSUM + tid] = t;
+    }
+}
+
+// Finalize for k_pot64p's partial rows: NSUM sums per row, summed in order.
+__global__ void __launch_bounds__(256) k_finalize_sums(const double* __restrict__ part, int nrows,
+                                                       double dv_norm, double dv_obs, double* out,
+                                                       int* counter, int max_rows, double* cur_norm,
+                                                       int* flag) {
+    __shared__ double S[NSUM];
+    if (threadIdx.x < NSUM) {
+        double t = 0.0;
+        for (int r = 0; r < nrows; ++r) t += part[(long long)r * NSUM + threadIdx.x];
+        S[threadIdx.x] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double2 n = make_double2(S[0] * dv_norm, S[1] * dv_norm);
+        const double2 inv = zinv(n);
+        auto obs = [&](int k) { return dv_obs * (S[k] * inv.x - S[k + 1] * inv.y); };
+        double row[WIG4D_NOBS];
+        row[0] = n.x; row[1] = n.y;
+        row[2] = obs(2); row[3] = obs(6); row[4] = obs(4); row[5] = obs(8);
+        row[6] = obs(10); row[7] = obs(14); row[8] = obs(12); row[9] = obs(16);
+        row[10] = dv_obs * ((S[18] + S[20]) * inv.x - (S[19] + S[21]) * inv.y);
+        double* dst = out;
+        if (counter) {
+            const int r = *counter;
+            dst = (r < max_rows) ? out + (long long)r * WIG4D_NOBS : nullptr;
+            *counter = r + 1;
+        }
+        bool bad = false;
+        for (int i = 0; i < WIG4D_NOBS; ++i) bad |= !isfinite(row[i]);
+        if (bad && flag) *flag = WIG_ERR_NONFINITE;
+        if (dst)
+            for (int i = 0; i < WIG4D_NOBS; ++i) dst[i] = row[i];
+        if (cur_norm) { cur_norm[0] = n.x; cur_norm[1] = n.y; }
     }
 }
 
@@ -388,6 +881,8 @@ struct wig4d_plan {
     double* cur_norm;              // complex128 norm of the current state
     int* counter;                  // history row of the next finalize
     int* flag;                     // WIG_ERR_NONFINITE when seen
+    bool fast64;                   // 64^4 grid: Run() uses k_kin64 / k_pot64
+    void* pingpong;                // second state buffer (layout [y][x][p_y][p_x])
     // CUDA graph of one Run() iteration, cached per (W, history, stream)
     cudaGraphExec_t graph;
     void* graph_W;
@@ -397,8 +892,9 @@ struct wig4d_plan {
 
 static bool pow2_16_128(int n) { return n == 16 || n == 32 || n == 64 || n == 128; }
 
-template <class C>
-static size_t plane_smem(int a, int b) { return sizeof(C) * ((size_t)a * b + a + b); }
+// Threads per CTA of the fused kernels: one radix-8 butterfly per thread and
+// pass for a 64 x 64 plane; smaller planes use fewer threads.
+template <int A, int B> struct FusedNT { static constexpr int v = (A * B / 8 >= 512) ? 512 : (A * B / 8 >= 256 ? 256 : 128); };
 
 template <class C> static FactorSet<C>& kin_set(wig4d_plan* p);
 template <> FactorSet<double2>& kin_set<double2>(wig4d_plan* p) { return p->kin_d; }
@@ -418,10 +914,11 @@ static int launch_kinetic(wig4d_plan* p, C* W, const double* d_norm, cudaStream_
     const double2 sc = make_double2(p->kin_scale, 0.0);
 #define KCASE(a, b)                                                                      \
     if (NY == a && NX == b) {                                                            \
-        auto kern = k_kinetic<C, a, b, 256>;                                             \
-        size_t sm = plane_smem<C>(a, b);                                                 \
+        constexpr int NT = FusedNT<a, b>::v;                                             \
+        auto kern = k_kinetic<C, a, b, NT>;                                              \
+        size_t sm = plane_bytes<C, a, b>();                                              \
         WIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
-        kern<<<grid, 256, sm, st>>>(W, npy, npx, kin_set<C>(p), sc, d_norm);             \
+        kern<<<grid, NT, sm, st>>>(W, npy, npx, kin_set<C>(p), sc, d_norm);              \
         WIG_LAUNCHED("k_kinetic");                                                       \
         return WIG_OK;                                                                   \
     }
@@ -438,11 +935,12 @@ static int launch_potential(wig4d_plan* p, C* W, double* partials, cudaStream_t 
     const double2 sc = make_double2(p->pot_scale, 0.0);
 #define PCASE(a, b)                                                                      \
     if (NPY == a && NPX == b) {                                                          \
-        auto kern = k_potential<C, a, b, 256>;                                           \
-        size_t sm = plane_smem<C>(a, b);                                                 \
-        if (sm < NPART * 8 * sizeof(double)) sm = NPART * 8 * sizeof(double);            \
+        constexpr int NT = FusedNT<a, b>::v;                                             \
+        auto kern = k_potential<C, a, b, NT>;                                            \
+        size_t sm = plane_bytes<C, a, b>();                                              \
+        if (sm < NPART * (NT / 32) * sizeof(double)) sm = NPART * (NT / 32) * sizeof(double); \
         WIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
-        kern<<<grid, 256, sm, st>>>(W, ny, nx, pot_set<C>(p), sc, p->ob, partials);      \
+        kern<<<grid, NT, sm, st>>>(W, ny, nx, pot_set<C>(p), sc, p->ob, partials);       \
         WIG_LAUNCHED("k_potential");                                                     \
         return WIG_OK;                                                                   \
     }
@@ -521,6 +1019,7 @@ static void free_plan(wig4d_plan* p) {
     cudaFree(p->obs_mem);
     cudaFree(p->partials);
     cudaFree(p->cur_norm);
+    cudaFree(p->pingpong);
     delete p;
 }
 
@@ -557,9 +1056,9 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
     const size_t esz = desc->dtype == WIG_C128 ? 16 : 8;
     const size_t max_smem = 227 * 1024;
     p->fused_kin = fast_axis(1) && fast_axis(3) &&
-                   esz * ((size_t)p->shape[1] * p->shape[3] + p->shape[1] + p->shape[3]) <= max_smem;
+                   esz * ((size_t)p->shape[1] * (p->shape[3] + 1) + p->shape[1] + p->shape[3]) <= max_smem;
     p->fused_pot = fast_axis(0) && fast_axis(2) &&
-                   esz * ((size_t)p->shape[0] * p->shape[2] + p->shape[0] + p->shape[2]) <= max_smem;
+                   esz * ((size_t)p->shape[0] * (p->shape[2] + 1) + p->shape[0] + p->shape[2]) <= max_smem;
     auto plane_ok = [](int a, int b) {
         return (a == b && pow2_16_128(a)) || (a == 64 && b == 128) || (a == 128 && b == 64);
     };
@@ -637,6 +1136,26 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
         const bool fast = pow2_16_128(p->shape[a]) && fabs(fabs(p->delta[a]) * p->shape[a] - 1.0) < 1e-12;
         if (!fast && !wig_dense_matrix(p->shape[a], fabs(p->delta[a]), p->dtype, 0)) { free_plan(p); return WIG_ERR_ALLOC; }
     }
+    p->fast64 = p->fused_kin && p->fused_pot && p->shape[0] == 64 && p->shape[1] == 64 &&
+                p->shape[2] == 64 && p->shape[3] == 64 && getenv("WIG_NO_FAST64") == nullptr;
+    if (p->fast64) {
+        if (cudaMalloc(&p->pingpong, (size_t)p->npts * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+        const int sm = (int)(esz * (64 * lanes64::LD + 64) + 2 * 64 * sizeof(double2));
+        if (desc->dtype == WIG_C128) {
+            cudaFuncSetAttribute(k_kin64p<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+            cudaFuncSetAttribute(k_pot64p<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        } else {
+            cudaFuncSetAttribute(k_kin64p<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+            cudaFuncSetAttribute(k_pot64p<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        }
+        // the persistent kernels write one NSUM row per CTA
+        if ((size_t)wig_num_sms() * NSUM > (size_t)p->shape[1] * p->shape[3] * NPART) {
+            cudaFree(p->partials);
+            if (cudaMalloc(&p->partials, (size_t)wig_num_sms() * NSUM * sizeof(double)) != cudaSuccess) {
+                free_plan(p); return WIG_ERR_ALLOC;
+            }
+        }
+    }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { wig_set_cuda_error(e, "wig4d_plan_create"); free_plan(p); return WIG_ERR_CUDA; }
     *out = p;
@@ -653,7 +1172,9 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 extern "C" long long wig4d_plan_device_bytes(const wig4d_plan* p) {
     if (!p) return -1;
     const long long N0 = p->shape[0], N1 = p->shape[1], N2 = p->shape[2], N3 = p->shape[3];
-    return p->tab_bytes + 8 * (N0 + N1 + N2 + N3 + N0 * N2 + N1 * N3) + 8LL * N1 * N3 * NPART + 32;
+    const long long esz = p->dtype == WIG_C128 ? 16 : 8;
+    return p->tab_bytes + 8 * (N0 + N1 + N2 + N3 + N0 * N2 + N1 * N3) + 8LL * N1 * N3 * NPART + 32 +
+           (p->pingpong ? p->npts * esz : 0);
 }
 
 extern "C" int wig4d_kinetic(wig4d_plan* p, void* W, const double* d_norm, void* stream) {
@@ -700,6 +1221,21 @@ extern "C" int wig4d_reduce(wig4d_plan* p, const void* W, double* d_out, void* s
 template <class C>
 static int iteration(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t st) {
     int s;
+    if (p->fast64) {
+        constexpr size_t sm = sizeof(C) * (64 * lanes64::LD + 64) + 2 * 64 * sizeof(double2);
+        C* T = reinterpret_cast<C*>(p->pingpong);
+        const int nsm = wig_num_sms();
+        k_kin64p<C><<<nsm, lanes64::NT, sm, st>>>(
+            W, T, p->shape[0], p->shape[2], kin_set<C>(p), make_double2(p->kin_scale, 0.0), p->cur_norm);
+        WIG_LAUNCHED("k_kin64p");
+        k_pot64p<C><<<nsm, lanes64::NT, sm, st>>>(
+            T, W, p->shape[1], p->shape[3], pot_set<C>(p), make_double2(p->pot_scale, 0.0), p->ob, p->partials);
+        WIG_LAUNCHED("k_pot64p");
+        k_finalize_sums<<<1, 256, 0, st>>>(p->partials, nsm, p->dv_norm, p->dv_obs, hist, p->counter, rows,
+                                          p->cur_norm, p->flag);
+        WIG_LAUNCHED("k_finalize_sums");
+        return WIG_OK;
+    }
     if ((s = kinetic_impl<C>(p, W, p->cur_norm, st))) return s;
     if ((s = potential_impl<C>(p, W, p->partials, st))) return s;
     return finalize(p, hist, p->counter, rows, st);

@@ -187,3 +187,38 @@ def test_nonfinite_state_raises():
     f.fileName = None
     with pytest.raises(FloatingPointError):
         f.Run()
+
+
+def test_run_fast64_vs_oracle():
+    """64^4 takes the register-resident ping-pong kernels (k_kin64 / k_pot64)."""
+    from configs import cat_xp
+    p, c = config2(0, 64)
+    f, o = _pair(p)
+    W0 = cat_xp(f._coords, c)
+    f.W_init_gpu.set(W0)
+    f.timeSteps = 2
+    f.fileName = None
+    f.Run()
+    Wo, obs = o.run(W0, 2)
+    for name in OBS:
+        assert rel_err(getattr(f, name), obs[name]) < 1e-12, name
+    assert rel_err(f.W_init_gpu.get(), Wo) < 1e-10
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-12), (np.complex64, 1e-5)])
+def test_fast64_matches_generic_kernels(dtype, tol, monkeypatch):
+    from configs import cat_xp
+    p, c = config2(3, 64)
+    f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    monkeypatch.setenv("WIG_NO_FAST64", "1")
+    f2 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    monkeypatch.delenv("WIG_NO_FAST64")
+    W0 = cat_xp(f1._coords, c).astype(dtype)
+    for f in (f1, f2):
+        f.W_init_gpu.set(W0)
+        f.timeSteps = 19
+        f.fileName = None
+        f.Run()
+    for name in OBS:
+        assert rel_err(getattr(f1, name), getattr(f2, name)) < tol, name
+    assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < 100 * tol
