@@ -96,7 +96,7 @@ int wig_real(void* data, long long n, int dtype, void* stream);
  * Host data is interleaved (re, im) float64; the plan copies it to the GPU
  * (rounded to complex64 for WIG_C64 plans).
  */
-#define WIG_MAX_FACTORS 6
+#define WIG_MAX_FACTORS 12
 typedef struct {
     int axis_a;
     int axis_b;

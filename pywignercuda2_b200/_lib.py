@@ -9,7 +9,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libwigner_b200.so")
 
-WIG_MAX_FACTORS = 6
+WIG_MAX_FACTORS = 12
 WIG4D_NOBS = 11
 C128, C64 = 0, 1
 

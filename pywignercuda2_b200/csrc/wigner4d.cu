@@ -424,268 +424,215 @@ __global__ void __launch_bounds__(lanes64::NT, 2) k_pot64(const C* __restrict__ 
 // ---------------------------------------------------------------------------
 #define NSUM 22   // sum W, xW, x^2 W, p_x W, p_x^2 W, yW, y^2 W, p_y W, p_y^2 W, K W, V W (complex)
 
+// Per-plane factor vectors, built once at plan creation: for plane (f0, f1)
+// the row-frequency vector PV[plane][0][k] and the column-frequency vector
+// PV[plane][1][k] (k already shifted by N/2), whose outer product is the
+// separable part of the factor.  Tables over both in-plane axes or full
+// tables stay per point (the kernels test `pp`).
 template <class C>
-struct PlaneFactors {
-    // in-plane axes (ay: the row index axis, ax: the column index axis) and
-    // the two fixed axes of the CTA's plane
-    int ay, ax;
-};
-
-// Build fy[0..63] (factor along the row-frequency axis, c0 folded in) and
-// fx[0..63] for the plane with fixed indices (fixed0 on axis f0, fixed1 on f1).
-// Tables over both in-plane axes or full 4-D tables set *per_point.
-template <class C>
-__device__ __forceinline__ void build_plane_factors(const FactorSet<C>& F, int ay, int ax, int f0, int i_f0,
-                                                    int f1, int i_f1, double2 c0, double2* fy, double2* fx) {
-    const int t = threadIdx.x;
-    if (t < 128) {
-        const bool along_y = t < 64;
-        const int k = t & 63;
-        const int kk = (k + 32) & 63;          // N/2-shifted frequency (see above)
-        const int axis = along_y ? ay : ax;
-        double2 acc = along_y ? c0 : make_double2(1.0, 0.0);
-        for (int j = 0; j < F.n; ++j) {
-            const int a = F.ia[j], b = F.ib[j];
-            if (a < 0) continue;                                  // full table: per point
-            const bool ina = (a == ay || a == ax), inb = (b >= 0) && (b == ay || b == ax);
-            if (ina && inb) continue;                             // both in-plane: per point
-            // scalar tables (no in-plane axis) go into fy only
-            const bool touches = (a == axis) || (b == axis);
-            const bool scalar = !ina && !inb;
-            if (!(touches || (scalar && along_y))) continue;
-            auto idx_of = [&](int ax_) { return ax_ == axis ? kk : (ax_ == f0 ? i_f0 : i_f1); };
-            long long idx = (b < 0) ? idx_of(a) : (long long)idx_of(a) * F.nb[j] + idx_of(b);
-            acc = zmul(acc, to_d2(F.data[j][idx]));
-        }
-        (along_y ? fy : fx)[k] = acc;
+__global__ void k_plane_vectors(FactorSet<C> F, int ay, int ax, int f0, int f1, int n_f1, int nplanes,
+                                C* __restrict__ PV) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)nplanes * 128) return;
+    const int plane = (int)(t >> 7), j = (int)(t & 127);
+    const bool along_y = j < 64;
+    const int k = j & 63, kk = (k + 32) & 63;
+    const int i_f0 = plane / n_f1, i_f1 = plane % n_f1;
+    const int axis = along_y ? ay : ax;
+    double2 acc = make_double2(1.0, 0.0);
+    for (int m = 0; m < F.n; ++m) {
+        const int a = F.ia[m], b = F.ib[m];
+        if (a < 0) continue;
+        const bool ina = (a == ay || a == ax), inb = (b >= 0) && (b == ay || b == ax);
+        if (ina && inb) continue;
+        const bool touches = (a == axis) || (b == axis);
+        const bool scalar = !ina && !inb;
+        if (!(touches || (scalar && along_y))) continue;
+        auto idx_of = [&](int ax_) { return ax_ == axis ? kk : (ax_ == f0 ? i_f0 : i_f1); };
+        const long long idx = (b < 0) ? idx_of(a) : (long long)idx_of(a) * F.nb[m] + idx_of(b);
+        acc = zmul(acc, to_d2(F.data[m][idx]));
     }
+    PV[t] = to_c<C>(acc);
 }
 
-template <class C>
-__device__ __forceinline__ bool has_per_point(const FactorSet<C>& F, int ay, int ax) {
-    for (int j = 0; j < F.n; ++j) {
-        const int a = F.ia[j], b = F.ib[j];
-        if (a < 0) return true;
-        if ((a == ay || a == ax) && b >= 0 && (b == ay || b == ax)) return true;
-    }
-    return false;
+// 32-byte store of two adjacent complex values (one full sector for c128)
+__device__ __forceinline__ void st_pair(double2* p, double2 a, double2 b) {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y)
+                 : "memory");
+}
+__device__ __forceinline__ void st_pair(float2* p, float2 a, float2 b) {
+    asm volatile("st.global.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y)
+                 : "memory");
 }
 
-// per-point part (only tables over both in-plane axes or full tables)
-template <class C>
-__device__ __forceinline__ C per_point_factor(const FactorSet<C>& F, int ay, int ax, int i0, int i1, int i2,
-                                              int i3, long long lin, C acc) {
-    for (int j = 0; j < F.n; ++j) {
-        const int a = F.ia[j], b = F.ib[j];
-        long long idx;
-        if (a < 0) idx = lin;
-        else if ((a == ay || a == ax) && b >= 0 && (b == ay || b == ax))
-            idx = (long long)sel4(a, i0, i1, i2, i3) * F.nb[j] + sel4(b, i0, i1, i2, i3);
-        else continue;
-        acc = cmul(acc, __ldg(F.data[j] + idx));
-    }
-    return acc;
+// The two half-steps share one body: a CTA loops over PAIRS of planes that
+// are neighbours in the destination's fastest index, transforms both, and
+// writes each destination point pair with one 32-byte store.
+//   KIN: src plane (p_y, p_x) of W (L0), dst T (L1 = [y][x][p_y][p_x]);
+//   POT: src plane (y, x) of T (contiguous), dst W (L0), plus observables.
+template <class C, bool KIN>
+__device__ __forceinline__ const C* half64_src_row(const C* base, int pl, int n_f1, int grp) {
+    if (KIN) return base + (((long long)(pl / n_f1) * 64 + grp) * n_f1 + pl % n_f1) * 64;
+    return base + ((long long)pl * 64 + grp) * 64;
 }
 
-template <class C>
-__global__ void __launch_bounds__(lanes64::NT, 1) k_kin64p(const C* __restrict__ W, C* __restrict__ T,
-                                                           int npy, int npx, FactorSet<C> F, double2 scale,
-                                                           const double* __restrict__ d_norm) {
-    using namespace lanes64;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* s = reinterpret_cast<C*>(smraw);
-    C* tw = s + 64 * LD;
-    double2* fy = reinterpret_cast<double2*>(tw + 64);
-    double2* fx = fy + 64;
-    const int tid = threadIdx.x, grp = tid >> 3, q = tid & 7, gi = grp & 3;
-    C* ws = s + (tid >> 5) * 4 * LD;
-    const int nplanes = npy * npx;
-    make_twiddles(tw, 64);
-    double2 c0 = scale;
-    if (d_norm) c0 = zmul(c0, zinv(make_double2(d_norm[0], d_norm[1])));
-    const bool pp = has_per_point(F, 1, 3);
-    const long long rs = (long long)npx * 64;   // stride of y in W
-    int plane = blockIdx.x;
-    C nv[8];
-    if (plane < nplanes) {
-        const C* src = W + (((long long)(plane / npx) * 64 + grp) * npx + plane % npx) * 64;
-#pragma unroll
-        for (int r = 0; r < 8; ++r) nv[r] = src[q + 8 * r];
-    }
-    for (; plane < nplanes; plane += gridDim.x) {
-        C v[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = nv[r];
-        const int next = plane + gridDim.x;
-        if (next < nplanes) {
-            const C* src = W + (((long long)(next / npx) * 64 + grp) * npx + next % npx) * 64;
-#pragma unroll
-            for (int r = 0; r < 8; ++r) nv[r] = src[q + 8 * r];
-        }
-        const int ipx = plane % npx, ipy = plane / npx;
-        build_plane_factors(F, 1, 3, 0, ipy, 2, ipx, c0, fy, fx);
-        __syncthreads();                                  // twiddles, factors; previous plane done
-        fft64<C, true>(v, ws, gi, q, tw);                 // along x: (y = grp, kx = q + 8 k)
-#pragma unroll
-        for (int k = 0; k < 8; ++k) s[grp * LD + q + 8 * k] = v[k];
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = s[(q + 8 * r) * LD + grp];
-        __syncthreads();
-        fft64<C, true>(v, ws, gi, q, tw);                 // along y: (ky = q + 8 k, kx = grp)
-        const C fxv = to_c<C>(fx[grp]);
-        const int kxs = (grp + 32) & 63;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            C f = cmul(to_c<C>(fy[q + 8 * k]), fxv);
-            if (pp) {
-                const int kys = (q + 8 * k + 32) & 63;
-                f = per_point_factor(F, 1, 3, ipy, kys, ipx, kxs,
-                                     (((long long)ipy * 64 + kys) * npx + ipx) * 64 + kxs, f);
-            }
-            v[k] = cmul(v[k], f);
-        }
-        fft64<C, false>(v, ws, gi, q, tw);                // (y = q + 8 k, kx = grp)
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < 8; ++k) s[(q + 8 * k) * LD + grp] = v[k];
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = s[grp * LD + q + 8 * r];
-        __syncthreads();
-        fft64<C, false>(v, ws, gi, q, tw);                // (y = grp, x = q + 8 k)
-        C* dst = T + ((long long)grp * 64 * npy + ipy) * npx + ipx;
-        const long long xs = (long long)npy * npx;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) dst[(q + 8 * k) * xs] = v[k];
-        (void)rs;
-    }
-}
-
-template <class C>
-__global__ void __launch_bounds__(lanes64::NT, 1) k_pot64p(const C* __restrict__ T, C* __restrict__ W,
-                                                           int ny, int nx, FactorSet<C> F, double2 scale,
+template <class C, bool KIN>
+__global__ void __launch_bounds__(lanes64::NT, 1) k_half64(const C* __restrict__ src_base, C* __restrict__ dst_base,
+                                                           int n_f0, int n_f1, const C* __restrict__ PV,
+                                                           double2 scale, const double* __restrict__ d_norm,
                                                            ObsTabs ob, double* __restrict__ partials) {
     using namespace lanes64;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* s = reinterpret_cast<C*>(smraw);
     C* tw = s + 64 * LD;
-    double2* fy = reinterpret_cast<double2*>(tw + 64);
-    double2* fx = fy + 64;
+    C* fv = tw + 64;                 // 128: row vector then column vector of the plane
+    C* hold = fv + 128;              // results of the first plane of a pair [k][tid]
+    double* red = reinterpret_cast<double*>(hold + 8 * lanes64::NT);   // POT: [12][NT] per-plane partials
+    double* acc = red + 12 * lanes64::NT + 16;                            // POT: NSUM running sums
     const int tid = threadIdx.x, grp = tid >> 3, q = tid & 7, gi = grp & 3;
     C* ws = s + (tid >> 5) * 4 * LD;
-    const int nplanes = ny * nx;
+    const int nplanes = n_f0 * n_f1, npairs = nplanes >> 1;
     make_twiddles(tw, 64);
-    const bool pp = has_per_point(F, 0, 2);
-    const long long pys = (long long)ny * 64 * nx;
-    double a[NSUM];
-#pragma unroll
-    for (int i = 0; i < NSUM; ++i) a[i] = 0.0;
-    const double qy = __ldg(ob.cpy + grp);
-    int plane = blockIdx.x;
+    double2 c0 = scale;
+    if (KIN && d_norm) c0 = zmul(c0, zinv(make_double2(d_norm[0], d_norm[1])));
+    const C cc = to_c<C>(c0);
+    // source row of plane pl for this thread: KIN -> W[((f0*64 + grp)*n_f1 + f1)*64 + x]
+    //                                         POT -> T[(pl*64 + grp)*64 + p_x]
+    if (!KIN && tid < NSUM) acc[tid] = 0.0;
+    int pair = blockIdx.x;
     C nv[8];
-    if (plane < nplanes) {
-        const C* src = T + ((long long)plane * 64 + grp) * 64;
+    C nf = mk<C>(0, 0);
+    if (pair < npairs) {
+        const C* r = half64_src_row<C, KIN>(src_base, 2 * pair, n_f1, grp);
 #pragma unroll
-        for (int r = 0; r < 8; ++r) nv[r] = src[q + 8 * r];
+        for (int i = 0; i < 8; ++i) nv[i] = r[q + 8 * i];
+        if (tid < 128) nf = PV[(long long)(2 * pair) * 128 + tid];
     }
-    for (; plane < nplanes; plane += gridDim.x) {
-        C v[8];
+    for (; pair < npairs; pair += gridDim.x) {
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+            const int pl = 2 * pair + h;
+            C v[8];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = nv[r];
-        const int next = plane + gridDim.x;
-        if (next < nplanes) {
-            const C* src = T + ((long long)next * 64 + grp) * 64;
+            for (int i = 0; i < 8; ++i) v[i] = nv[i];
+            const C cur_f = nf;
+            const int next = h == 0 ? pl + 1 : 2 * (pair + gridDim.x);
+            if (next < nplanes) {
+                const C* r = half64_src_row<C, KIN>(src_base, next, n_f1, grp);
 #pragma unroll
-            for (int r = 0; r < 8; ++r) nv[r] = src[q + 8 * r];
-        }
-        const int ix = plane % nx, iy = plane / nx;
-        build_plane_factors(F, 0, 2, 1, iy, 3, ix, scale, fy, fx);
-        __syncthreads();
-        fft64<C, true>(v, ws, gi, q, tw);                 // along p_x
-#pragma unroll
-        for (int k = 0; k < 8; ++k) s[grp * LD + q + 8 * k] = v[k];
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = s[(q + 8 * r) * LD + grp];
-        __syncthreads();
-        fft64<C, true>(v, ws, gi, q, tw);                 // along p_y: (theta_y = q + 8 k, theta_x = grp)
-        const C fxv = to_c<C>(fx[grp]);
-        const int kxs = (grp + 32) & 63;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            C f = cmul(to_c<C>(fy[q + 8 * k]), fxv);
-            if (pp) {
-                const int kys = (q + 8 * k + 32) & 63;
-                f = per_point_factor(F, 0, 2, kys, iy, kxs, ix,
-                                     (((long long)kys * ny + iy) * 64 + kxs) * nx + ix, f);
+                for (int i = 0; i < 8; ++i) nv[i] = r[q + 8 * i];
+                if (tid < 128) nf = PV[(long long)next * 128 + tid];
             }
-            v[k] = cmul(v[k], f);
+            const int f0 = pl / n_f1, f1 = pl % n_f1;
+            __syncthreads();                              // previous plane done with smem
+            if (tid < 128) fv[tid] = cur_f;
+            fft64<C, true>(v, ws, gi, q, tw);             // rows: (row = grp, kcol = q + 8 k)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) s[grp * LD + q + 8 * k] = v[k];
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[r] = s[(q + 8 * r) * LD + grp];
+            __syncthreads();
+            fft64<C, true>(v, ws, gi, q, tw);             // columns: (krow = q + 8 k, kcol = grp)
+            const C fx = cmul(fv[64 + grp], cc);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = cmul(v[k], cmul(fv[q + 8 * k], fx));
+            fft64<C, false>(v, ws, gi, q, tw);
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < 8; ++k) s[(q + 8 * k) * LD + grp] = v[k];
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[r] = s[grp * LD + q + 8 * r];
+            __syncthreads();
+            fft64<C, false>(v, ws, gi, q, tw);            // (row = grp, col = q + 8 k)
+            if (!KIN) {
+                // observables of the new (x, p) state (rows p_y = grp, columns p_x):
+                // per-thread partials -> smem -> 12 warps reduce one double each
+                // in a fixed order -> running sums with the plane's x, y, V(x, y)
+                double sw0 = 0.0, sw1 = 0.0, sx0 = 0.0, sx1 = 0.0, sxx0 = 0.0, sxx1 = 0.0, sk0 = 0.0, sk1 = 0.0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int px = q + 8 * k;
+                    const double2 w = to_d2(v[k]);
+                    const double qx = __ldg(ob.cpx + px), kk = __ldg(ob.ep + grp * 64 + px);
+                    sw0 += w.x; sw1 += w.y;
+                    sx0 = fma(qx, w.x, sx0); sx1 = fma(qx, w.y, sx1);
+                    sxx0 = fma(qx * qx, w.x, sxx0); sxx1 = fma(qx * qx, w.y, sxx1);
+                    sk0 = fma(kk, w.x, sk0); sk1 = fma(kk, w.y, sk1);
+                }
+                const double qy = __ldg(ob.cpy + grp);
+                red[0 * NT + tid] = sw0;            red[1 * NT + tid] = sw1;
+                red[2 * NT + tid] = qy * sw0;       red[3 * NT + tid] = qy * sw1;
+                red[4 * NT + tid] = qy * qy * sw0;  red[5 * NT + tid] = qy * qy * sw1;
+                red[6 * NT + tid] = sx0;            red[7 * NT + tid] = sx1;
+                red[8 * NT + tid] = sxx0;           red[9 * NT + tid] = sxx1;
+                red[10 * NT + tid] = sk0;           red[11 * NT + tid] = sk1;
+                __syncthreads();
+                const int w = tid >> 5, l = tid & 31;
+                if (w < 12) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int i = 0; i < NT / 32; ++i) t += red[w * NT + i * 32 + l];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+                    if (l == 0) red[12 * NT + w] = t;   // scratch slots after the partials... see acc below
+                }
+                __syncthreads();
+                if (tid < 2) {   // tid 0: real parts, tid 1: imaginary parts
+                    const double* P = red + 12 * NT;
+                    const double x = __ldg(ob.cx + f1), y = __ldg(ob.cy + f0), V = __ldg(ob.ex + f0 * n_f1 + f1);
+                    const double W0 = P[0 + tid], Wy = P[2 + tid], Wyy = P[4 + tid];
+                    const double Wx = P[6 + tid], Wxx = P[8 + tid], Wk = P[10 + tid];
+                    acc[0 + tid] += W0;                 // sum W
+                    acc[2 + tid] += x * W0;             // x W
+                    acc[4 + tid] += x * x * W0;         // x^2 W
+                    acc[6 + tid] += Wx;                 // p_x W
+                    acc[8 + tid] += Wxx;                // p_x^2 W
+                    acc[10 + tid] += y * W0;            // y W
+                    acc[12 + tid] += y * y * W0;        // y^2 W
+                    acc[14 + tid] += Wy;                // p_y W
+                    acc[16 + tid] += Wyy;               // p_y^2 W
+                    acc[18 + tid] += Wk;                // K W
+                    acc[20 + tid] += V * W0;            // V W
+                }
+            }
+            if (h == 0) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) hold[k * NT + tid] = v[k];
+            } else {
+                // destination of (row = grp, col = c) for the plane pair (f0, f1 - 1 .. f1)
+                //   KIN: T[((y*64 + x)*n_f0 + p_y)*n_f1 + p_x] with y = grp, x = c, p_y = f0, p_x = f1
+                //   POT: W[((p_y*n_f0 + y)*64 + p_x)*n_f1 + x] with p_y = grp, p_x = c, y = f0, x = f1
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int c = q + 8 * k;
+                    const long long di = KIN ? (((long long)grp * 64 + c) * n_f0 + f0) * n_f1 + (f1 - 1)
+                                             : (((long long)grp * n_f0 + f0) * 64 + c) * n_f1 + (f1 - 1);
+                    st_pair(dst_base + di, hold[k * NT + tid], v[k]);
+                }
+            }
         }
-        fft64<C, false>(v, ws, gi, q, tw);
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < 8; ++k) s[(q + 8 * k) * LD + grp] = v[k];
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < 8; ++r) v[r] = s[grp * LD + q + 8 * r];
-        __syncthreads();
-        fft64<C, false>(v, ws, gi, q, tw);                // (p_y = grp, p_x = q + 8 k)
-        C* dst = W + (long long)grp * pys + (long long)iy * 64 * nx + ix;
-        double sw0 = 0.0, sw1 = 0.0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int px = q + 8 * k;
-            dst[(long long)px * nx] = v[k];
-            const double2 w = to_d2(v[k]);
-            const double qx = __ldg(ob.cpx + px), kk = __ldg(ob.ep + grp * 64 + px);
-            sw0 += w.x; sw1 += w.y;
-            a[6] = fma(qx, w.x, a[6]); a[7] = fma(qx, w.y, a[7]);
-            a[8] = fma(qx * qx, w.x, a[8]); a[9] = fma(qx * qx, w.y, a[9]);
-            a[18] = fma(kk, w.x, a[18]); a[19] = fma(kk, w.y, a[19]);
-        }
-        const double x = __ldg(ob.cx + ix), y = __ldg(ob.cy + iy), V = __ldg(ob.ex + iy * nx + ix);
-        a[0] += sw0; a[1] += sw1;
-        a[2] = fma(x, sw0, a[2]); a[3] = fma(x, sw1, a[3]);
-        a[4] = fma(x * x, sw0, a[4]); a[5] = fma(x * x, sw1, a[5]);
-        a[10] = fma(y, sw0, a[10]); a[11] = fma(y, sw1, a[11]);
-        a[12] = fma(y * y, sw0, a[12]); a[13] = fma(y * y, sw1, a[13]);
-        a[14] = fma(qy, sw0, a[14]); a[15] = fma(qy, sw1, a[15]);
-        a[16] = fma(qy * qy, sw0, a[16]); a[17] = fma(qy * qy, sw1, a[17]);
-        a[20] = fma(V, sw0, a[20]); a[21] = fma(V, sw1, a[21]);
     }
-    // block reduction of NSUM doubles (fixed order)
-#pragma unroll
-    for (int i = 0; i < NSUM; ++i) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) a[i] += __shfl_down_sync(0xffffffffu, a[i], o);
-    }
-    __syncthreads();
-    double* sm = reinterpret_cast<double*>(smraw);
-    const int w = tid >> 5, l = tid & 31;
-    if (l == 0) {
-#pragma unroll
-        for (int i = 0; i < NSUM; ++i) sm[w * NSUM + i] = a[i];
-    }
-    __syncthreads();
-    if (tid < NSUM) {
-        double t = 0.0;
-        for (int k = 0; k < NT / 32; ++k) t += sm[k * NSUM + tid];
-        partials[(long long)blockIdx.x * NSUM + tid] = t;
+    if (!KIN) {
+        __syncthreads();
+        if (tid < NSUM) partials[(long long)blockIdx.x * NSUM + tid] = acc[tid];
     }
 }
 
-// Finalize for k_pot64p's partial rows: NSUM sums per row, summed in order.
-__global__ void __launch_bounds__(256) k_finalize_sums(const double* __restrict__ part, int nrows,
-                                                       double dv_norm, double dv_obs, double* out,
-                                                       int* counter, int max_rows, double* cur_norm,
-                                                       int* flag) {
+// Finalize for k_half64<pot>'s partial rows: NSUM sums per row.  One warp
+// per sum: lanes stride over the rows, then a fixed shuffle tree.
+__global__ void __launch_bounds__(32 * NSUM) k_finalize_sums(const double* __restrict__ part, int nrows,
+                                                            double dv_norm, double dv_obs, double* out,
+                                                            int* counter, int max_rows, double* cur_norm,
+                                                            int* flag) {
     __shared__ double S[NSUM];
-    if (threadIdx.x < NSUM) {
-        double t = 0.0;
-        for (int r = 0; r < nrows; ++r) t += part[(long long)r * NSUM + threadIdx.x];
-        S[threadIdx.x] = t;
-    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    double t = 0.0;
+    for (int r = l; r < nrows; r += 32) t += part[(long long)r * NSUM + w];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (l == 0) S[w] = t;
     __syncthreads();
     if (threadIdx.x == 0) {
         const double2 n = make_double2(S[0] * dv_norm, S[1] * dv_norm);
@@ -883,6 +830,7 @@ struct wig4d_plan {
     int* flag;                     // WIG_ERR_NONFINITE when seen
     bool fast64;                   // 64^4 grid: Run() uses k_kin64 / k_pot64
     void* pingpong;                // second state buffer (layout [y][x][p_y][p_x])
+    void* pv;                      // per-plane factor vectors of the two half-steps
     // CUDA graph of one Run() iteration, cached per (W, history, stream)
     cudaGraphExec_t graph;
     void* graph_W;
@@ -1020,6 +968,7 @@ static void free_plan(wig4d_plan* p) {
     cudaFree(p->partials);
     cudaFree(p->cur_norm);
     cudaFree(p->pingpong);
+    cudaFree(p->pv);
     delete p;
 }
 
@@ -1136,17 +1085,39 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
         const bool fast = pow2_16_128(p->shape[a]) && fabs(fabs(p->delta[a]) * p->shape[a] - 1.0) < 1e-12;
         if (!fast && !wig_dense_matrix(p->shape[a], fabs(p->delta[a]), p->dtype, 0)) { free_plan(p); return WIG_ERR_ALLOC; }
     }
+    // the 64^4 kernels take the factor as per-plane outer products: no full
+    // 4-D table and no table over both in-plane axes of a half-step
+    auto separable = [](const wig_factor* f, int n, int ay, int ax) {
+        for (int i = 0; i < n; ++i) {
+            if (f[i].axis_a < 0) return false;
+            const bool ina = f[i].axis_a == ay || f[i].axis_a == ax;
+            const bool inb = f[i].axis_b >= 0 && (f[i].axis_b == ay || f[i].axis_b == ax);
+            if (ina && inb) return false;
+        }
+        return true;
+    };
     p->fast64 = p->fused_kin && p->fused_pot && p->shape[0] == 64 && p->shape[1] == 64 &&
-                p->shape[2] == 64 && p->shape[3] == 64 && getenv("WIG_NO_FAST64") == nullptr;
+                p->shape[2] == 64 && p->shape[3] == 64 && separable(desc->kin, desc->n_kin, 1, 3) &&
+                separable(desc->pot, desc->n_pot, 0, 2) && getenv("WIG_NO_FAST64") == nullptr;
     if (p->fast64) {
         if (cudaMalloc(&p->pingpong, (size_t)p->npts * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
-        const int sm = (int)(esz * (64 * lanes64::LD + 64) + 2 * 64 * sizeof(double2));
+        const int sm = (int)(esz * (64 * lanes64::LD + 64 + 128 + 8 * lanes64::NT) + sizeof(double) * (12 * lanes64::NT + 16 + NSUM));
+        const int npl_k = p->shape[0] * p->shape[2], npl_p = p->shape[1] * p->shape[3];
+        if (cudaMalloc(&p->pv, (size_t)(npl_k + npl_p) * 128 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
         if (desc->dtype == WIG_C128) {
-            cudaFuncSetAttribute(k_kin64p<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-            cudaFuncSetAttribute(k_pot64p<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+            cudaFuncSetAttribute(k_half64<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+            cudaFuncSetAttribute(k_half64<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+            double2* pv = (double2*)p->pv;
+            k_plane_vectors<double2><<<(npl_k * 128 + 255) / 256, 256>>>(p->kin_d, 1, 3, 0, 2, p->shape[2], npl_k, pv);
+            k_plane_vectors<double2><<<(npl_p * 128 + 255) / 256, 256>>>(p->pot_d, 0, 2, 1, 3, p->shape[3], npl_p,
+                                                                        pv + (size_t)npl_k * 128);
         } else {
-            cudaFuncSetAttribute(k_kin64p<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-            cudaFuncSetAttribute(k_pot64p<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+            cudaFuncSetAttribute(k_half64<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+            cudaFuncSetAttribute(k_half64<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+            float2* pv = (float2*)p->pv;
+            k_plane_vectors<float2><<<(npl_k * 128 + 255) / 256, 256>>>(p->kin_f, 1, 3, 0, 2, p->shape[2], npl_k, pv);
+            k_plane_vectors<float2><<<(npl_p * 128 + 255) / 256, 256>>>(p->pot_f, 0, 2, 1, 3, p->shape[3], npl_p,
+                                                                       pv + (size_t)npl_k * 128);
         }
         // the persistent kernels write one NSUM row per CTA
         if ((size_t)wig_num_sms() * NSUM > (size_t)p->shape[1] * p->shape[3] * NPART) {
@@ -1222,16 +1193,18 @@ template <class C>
 static int iteration(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t st) {
     int s;
     if (p->fast64) {
-        constexpr size_t sm = sizeof(C) * (64 * lanes64::LD + 64) + 2 * 64 * sizeof(double2);
+        constexpr size_t sm = sizeof(C) * (64 * lanes64::LD + 64 + 128 + 8 * lanes64::NT) + sizeof(double) * (12 * lanes64::NT + 16 + NSUM);
         C* T = reinterpret_cast<C*>(p->pingpong);
         const int nsm = wig_num_sms();
-        k_kin64p<C><<<nsm, lanes64::NT, sm, st>>>(
-            W, T, p->shape[0], p->shape[2], kin_set<C>(p), make_double2(p->kin_scale, 0.0), p->cur_norm);
-        WIG_LAUNCHED("k_kin64p");
-        k_pot64p<C><<<nsm, lanes64::NT, sm, st>>>(
-            T, W, p->shape[1], p->shape[3], pot_set<C>(p), make_double2(p->pot_scale, 0.0), p->ob, p->partials);
-        WIG_LAUNCHED("k_pot64p");
-        k_finalize_sums<<<1, 256, 0, st>>>(p->partials, nsm, p->dv_norm, p->dv_obs, hist, p->counter, rows,
+        const C* pvk = reinterpret_cast<const C*>(p->pv);
+        const C* pvp = pvk + (size_t)p->shape[0] * p->shape[2] * 128;
+        k_half64<C, true><<<nsm, lanes64::NT, sm, st>>>(W, T, p->shape[0], p->shape[2], pvk,
+                                                        make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr);
+        WIG_LAUNCHED("k_half64<kin>");
+        k_half64<C, false><<<nsm, lanes64::NT, sm, st>>>(T, W, p->shape[1], p->shape[3], pvp,
+                                                         make_double2(p->pot_scale, 0.0), nullptr, p->ob, p->partials);
+        WIG_LAUNCHED("k_half64<pot>");
+        k_finalize_sums<<<1, 32 * NSUM, 0, st>>>(p->partials, nsm, p->dv_norm, p->dv_obs, hist, p->counter, rows,
                                           p->cur_norm, p->flag);
         WIG_LAUNCHED("k_finalize_sums");
         return WIG_OK;
