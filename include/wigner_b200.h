@@ -176,6 +176,86 @@ int wig4d_init_gaussian(wig4d_plan* plan, void* W, double mu_p_y, double mu_y,
 /* Bytes of device memory the plan holds (tables, partial sums). */
 long long wig4d_plan_device_bytes(const wig4d_plan* plan);
 
+/* ---- 4 x 4 spinor Wigner-Dirac / KvN plan -------------------------------- */
+/*
+ * The sixteen components W11..W44 are passed as an array of sixteen device
+ * pointers ("slots", row-major: slot 4a+b is W_{a+1,b+1}), each a 4-D array
+ * of the plan's shape.  The elementwise entry points (mask, real, divide,
+ * kinetic, potential, reduce, init) keep the reference's per-point order
+ * and accept repeated pointers, reproducing the reference's Run(), which
+ * binds W21 to W22 (GPU_WignerDirac4D.py:1716).  wigd_transform and
+ * wigd_run reject repeated pointers (WIG_ERR_ALIAS).
+ */
+typedef struct wigd_plan wigd_plan;
+
+typedef struct {
+    int shape[4];              /* N_py, N_y, N_px, N_x                            */
+    int dtype;                 /* WIG_C128 or WIG_C64                             */
+    int kvn;                   /* 0: GPU_WignerDirac4D, 1: GPU_WignerDiracKvN4D   */
+    double d[4], delta[4];     /* FAFT (d, delta) per axis, forward sign           */
+    double post[4];            /* divisors of X->Lambda, Lambda->X, P->Theta,
+                                  Theta->P (GPU_WignerDirac4D.py:1428-1458)       */
+    double c, hbar, mass, dt;  /* device constants (as the CUDA preamble has them) */
+    double m_pot;              /* mass of the potential propagator: 1e-12 Dirac
+                                  (WD4D:542), 1e-6 KvN (KvN:536)                  */
+    double d_lambda_x, d_lambda_y;   /* kinetic dephasing (WD4D:403)               */
+    const double* coord[4];    /* (x, p) grid: p_y, y, p_x, x                      */
+    const double* acoord[4];   /* ambiguity grid: theta_y, lambda_y, theta_x, lambda_x */
+    const double* mask_xp[4];  /* boundary_xp_GPU factor per axis (WD4D:327-366)   */
+    const double* mask_p[4];   /* boundary_p_GPU factor per axis (WD4D:292-325)    */
+    int n_phase;               /* A0 Bopp phase exp(-i dt (A0(x-) - A0(x+))/hbar)   */
+    wig_factor phase[WIG_MAX_FACTORS];   /* over (theta_y, y, theta_x, x)          */
+    int a_rank;                /* A1, A2, A3 at x -+ theta/2 as sums of a_rank     */
+    const double* a_tabs;      /* products F(ix, itheta_x) G(iy, itheta_y):
+                                  [3][2 sides][a_rank][N_x*N_px + N_y*N_py]        */
+    const double* obs_xy;      /* [7][N_y][N_x]: A0 A1 A2 A3 D1A0 D1A1 D1A2        */
+    double dv_norm, dv_obs;
+} wigd_desc;
+
+/* values per observables row: norm_re, norm_im, <x>, <p_x>, <x^2>, <p_x^2>, <y>,
+   <p_y>, <y^2>, <p_y^2>, Alpha_1, Alpha_2, Alpha_1_x, Alpha_2_y, energyKinetic,
+   energyPotential, D_1_A_0, D_1_A_1, D_1_A_2 (GPU_WignerDirac4D.py:1784-1822). */
+#define WIGD_NOBS 19
+
+int wigd_plan_create(const wigd_desc* desc, wigd_plan** plan);
+int wigd_plan_destroy(wigd_plan* plan);
+/* which: 0 X->Lambda, 1 Lambda->X, 2 P->Theta, 3 Theta->P on nslots
+   components (Fourier_*_64_64_4x4_GPU); d_norm (optional): complex128
+   device scalar divided out. */
+int wigd_transform(wigd_plan* plan, void* const* slots, int nslots, int which,
+                   const double* d_norm, void* stream);
+/* kind 1: boundary_xp_GPU, 2: boundary_p_GPU. */
+int wigd_mask(wigd_plan* plan, void* const* slots, int kind, void* stream);
+/* replace the factors of mask `kind` (four host float64 vectors, one per axis,
+   e.g. for other bound_x / bound_p values); synchronous. */
+int wigd_set_mask(wigd_plan* plan, int kind, const double* const* factors);
+/* Real_GPU on W11, W22, W33, W44. */
+int wigd_real_diag(wigd_plan* plan, void* const* slots, void* stream);
+/* every slot /= *d_norm, slot by slot (Normalize_4x4_GPU). */
+int wigd_divide(wigd_plan* plan, void* const* slots, const double* d_norm, void* stream);
+/* trace norm and observables into d_out[WIGD_NOBS]; divide != 0 divides the
+   observables by the norm.  The norm also goes to the plan's device scalar
+   (wigd_norm_ptr). */
+int wigd_reduce(wigd_plan* plan, void* const* slots, double* d_out, int divide, void* stream);
+const double* wigd_norm_ptr(wigd_plan* plan);
+/* ParticleProjector_GPU(sign) when projector_sign != 0, then the kinetic
+   sandwich exp_p_lambda_GPU when kinetic != 0, on the (lambda, p) grid. */
+int wigd_kinetic(wigd_plan* plan, void* const* slots, int projector_sign, int kinetic, void* stream);
+/* Potential_Propagator_Kernel on the (x, theta) grid. */
+int wigd_potential(wigd_plan* plan, void* const* slots, void* stream);
+/* initial states on the (x, theta) grid (GPU_WignerDirac4D.py:908-1032) */
+int wigd_init_particle_up(wigd_plan* plan, void* const* slots, double u_x, double u_y,
+                          double x_mu, double y_mu, double x_sigma, double y_sigma, void* stream);
+int wigd_init_majorana(wigd_plan* plan, void* const* slots, double u_x, double u_y,
+                       double x_mu, double y_mu, double x_sigma, double y_sigma, void* stream);
+int wigd_init_landau(wigd_plan* plan, void* const* slots, double B, double x_offset,
+                     double y_offset, void* stream);
+/* Run() (GPU_WignerDirac4D.py:1767-1851) with distinct component pointers:
+   iterations x {boundary_xp, Real, normalise + observables row, X->Lambda,
+   [projector], kinetic, Lambda->X, P->Theta, potential, Theta->P}. */
+int wigd_run(wigd_plan* plan, void* const* slots, int iterations, int filter,
+             double* d_history, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

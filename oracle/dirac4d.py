@@ -40,11 +40,14 @@ class DiracOracle:
     ``kvn=True`` selects the GPU_WignerDiracKvN4D variant.
     """
 
-    def __init__(self, params, kvn=False, round_constants=True):
+    def __init__(self, params, kvn=False, round_constants=True, a3_mode="sin_a3"):
         for k, v in params.items():
             setattr(self, k, v)
         self.kvn = kvn
         self.rc = round_constants
+        # "sin_a3": U13 = i sin(A3 c dt) as committed (GPU_WignerDirac4D.py:601-604);
+        # "sinF": the commented-out form i A3 sin(c dt F / hbar) / F (WD4D:596-599)
+        self.a3_mode = a3_mode
         self.dp_y = 2 * self.p_y_amplitude / float(self.gridDIM_p_y)
         self.dy = 2 * self.y_amplitude / float(self.gridDIM_y)
         self.dp_x = 2 * self.p_x_amplitude / float(self.gridDIM_p_x)
@@ -216,7 +219,7 @@ class DiracOracle:
         u23 = -(-A2 + 1j * A1) * s / F
         u32 = -(A2 + 1j * A1) * s / F
         u41 = (-A2 + 1j * A1) * s / F
-        s3 = np.sin(A3 * c * dt)
+        s3 = np.sin(A3 * c * dt) if self.a3_mode == "sin_a3" else A3 * s / F
         u13 = 1j * s3 + z
         u24 = -1j * s3 + z
         return [[u11, None, u13, u14], [None, u11, u23, u24], [u13, u32, u33, None],

@@ -11,10 +11,7 @@ from ._lib import WignerError, load as load_library  # noqa: F401
 from .device import DeviceScalar, GPUArray  # noqa: F401
 from .wigner4d import GPU_Wigner4D  # noqa: F401
 
-__all__ = ["GPU_Wigner4D", "GPUArray", "DeviceScalar", "WignerError", "load_library"]
+from .dirac4d import GPU_WignerDirac4D, GPU_WignerDiracKvN4D  # noqa: F401
 
-try:  # the Dirac classes (same package)
-    from .dirac4d import GPU_WignerDirac4D, GPU_WignerDiracKvN4D  # noqa: F401
-    __all__ += ["GPU_WignerDirac4D", "GPU_WignerDiracKvN4D"]
-except ImportError:  # pragma: no cover - module added in a later step
-    pass
+__all__ = ["GPU_Wigner4D", "GPU_WignerDirac4D", "GPU_WignerDiracKvN4D", "GPUArray", "DeviceScalar",
+           "WignerError", "load_library"]

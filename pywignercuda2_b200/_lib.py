@@ -46,6 +46,24 @@ class Desc4D(ctypes.Structure):
                 ("dv_norm", ctypes.c_double), ("dv_obs", ctypes.c_double)]
 
 
+class DescDirac(ctypes.Structure):
+    _fields_ = [("shape", ctypes.c_int * 4), ("dtype", ctypes.c_int), ("kvn", ctypes.c_int),
+                ("d", ctypes.c_double * 4), ("delta", ctypes.c_double * 4), ("post", ctypes.c_double * 4),
+                ("c", ctypes.c_double), ("hbar", ctypes.c_double), ("mass", ctypes.c_double),
+                ("dt", ctypes.c_double), ("m_pot", ctypes.c_double),
+                ("d_lambda_x", ctypes.c_double), ("d_lambda_y", ctypes.c_double),
+                ("coord", ctypes.POINTER(ctypes.c_double) * 4),
+                ("acoord", ctypes.POINTER(ctypes.c_double) * 4),
+                ("mask_xp", ctypes.POINTER(ctypes.c_double) * 4),
+                ("mask_p", ctypes.POINTER(ctypes.c_double) * 4),
+                ("n_phase", ctypes.c_int), ("phase", Factor * WIG_MAX_FACTORS),
+                ("a_rank", ctypes.c_int), ("a_tabs", ctypes.POINTER(ctypes.c_double)),
+                ("obs_xy", ctypes.POINTER(ctypes.c_double)),
+                ("dv_norm", ctypes.c_double), ("dv_obs", ctypes.c_double)]
+
+
+WIGD_NOBS = 19
+
 _lib = None
 
 _P = ctypes.c_void_p
@@ -78,9 +96,24 @@ SIGNATURES = {
     "wig4d_init_ho_ground": [_P, _P, _D, _D, _D, _D, _D, _D, _D, _P],
     "wig4d_init_gaussian": [_P, _P, _D, _D, _D, _D, _D, _D, _D, _D, _P],
     "wig4d_plan_device_bytes": [_P],
+    "wigd_plan_create": [ctypes.POINTER(DescDirac), ctypes.POINTER(_P)],
+    "wigd_plan_destroy": [_P],
+    "wigd_transform": [_P, _P, _I, _I, _P, _P],
+    "wigd_mask": [_P, _P, _I, _P],
+    "wigd_set_mask": [_P, _I, _P],
+    "wigd_real_diag": [_P, _P, _P],
+    "wigd_divide": [_P, _P, _P, _P],
+    "wigd_reduce": [_P, _P, _P, _I, _P],
+    "wigd_norm_ptr": [_P],
+    "wigd_kinetic": [_P, _P, _I, _I, _P],
+    "wigd_potential": [_P, _P, _P],
+    "wigd_init_particle_up": [_P, _P, _D, _D, _D, _D, _D, _D, _P],
+    "wigd_init_majorana": [_P, _P, _D, _D, _D, _D, _D, _D, _P],
+    "wigd_init_landau": [_P, _P, _D, _D, _D, _P],
+    "wigd_run": [_P, _P, _I, _I, _P, _P],
 }
 _RESTYPE = {"wig_status_string": ctypes.c_char_p, "wig_last_error": ctypes.c_char_p,
-            "wig4d_plan_device_bytes": ctypes.c_longlong}
+            "wig4d_plan_device_bytes": ctypes.c_longlong, "wigd_norm_ptr": ctypes.c_void_p}
 
 
 def load():

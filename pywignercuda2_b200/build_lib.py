@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                "-I", INCLUDE, "-I", CSRC, "--expt-relaxed-constexpr"]
+                "-I", INCLUDE, "-I", CSRC, "--expt-relaxed-constexpr", "-diag-suppress", "128"]
 
 
 def _sources():

@@ -1,0 +1,175 @@
+"""GPU parity of the Wigner-Dirac / KvN path against the NumPy oracle.
+
+complex128 must match the oracle to 1e-12 relative (max over components of
+max|dW| / max|W| for single kernels, 1e-11 after several Run() iterations),
+and the golden notebook norms to the digits the notebooks print.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from frames import make_frame, rel_err  # noqa: E402
+from golden.notebook_configs import NOTEBOOKS  # noqa: E402
+from oracle.dirac4d import DiracOracle  # noqa: E402
+from pywignercuda2_b200 import GPU_WignerDirac4D, GPU_WignerDiracKvN4D  # noqa: E402
+from pywignercuda2_b200.dirac4d import NAMES  # noqa: E402
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "notebook_norms.json")))
+
+
+def small(n=16, kvn=False, fast=False, **kw):
+    """A small frame: notebook-like windows (delta N != 1, dense path) or,
+    with fast, delta = 1/N windows (radix path)."""
+    amp_x, amp_p = 8.0, 2.5
+    p = dict(gridDIM_p_y=n, gridDIM_y=n, gridDIM_p_x=n, gridDIM_x=n, dt=0.01,
+             p_y_amplitude=amp_p, y_amplitude=amp_x, p_x_amplitude=amp_p, x_amplitude=amp_x,
+             theta_y_amplitude=20.0, lambda_y_amplitude=5.0, theta_x_amplitude=20.0,
+             lambda_x_amplitude=5.0, c=1.0, HBar=1.0, mass=1.0,
+             potential_0_String="0.3*(x*x + y*y)", potential_1_String="-0.2*y/2.",
+             potential_2_String="0.2*x/2.", potential_3_String="0." if kvn else "y*(x+16)/50.",
+             D_1_potential_0_String="0.6*x", D_1_potential_1_String="0.",
+             D_1_potential_2_String="0.1", D_theta_x=1e-3, D_theta_y=1e-3, D_lambda_x=2e-3,
+             D_lambda_y=1e-3)
+    if fast:
+        dx, dp = 2 * amp_x / n, 2 * amp_p / n
+        p.update(theta_x_amplitude=np.pi / dp, theta_y_amplitude=np.pi / dp,
+                 lambda_x_amplitude=np.pi / dx, lambda_y_amplitude=np.pi / dx)
+    p.update(kw)
+    return p
+
+
+def pair(params, kvn=False, **extra):
+    cls = GPU_WignerDiracKvN4D if kvn else GPU_WignerDirac4D
+    f = make_frame(cls, params, **extra)
+    o = DiracOracle(params, kvn=kvn)
+    return f, o
+
+
+def comps(f):
+    return [getattr(f, n).get() for n in NAMES]
+
+
+def err16(a, b):
+    scale = max(np.max(np.abs(x)) for x in b)
+    return max(np.max(np.abs(x - y)) for x, y in zip(a, b)) / scale
+
+
+def set_state(f, o, seed=0):
+    rng = np.random.default_rng(seed)
+    for k, n in enumerate(NAMES):
+        v = (rng.standard_normal(f.shape) + 1j * rng.standard_normal(f.shape)) * np.exp(-0.3 * k)
+        getattr(f, n).set(v)
+        o.W[k][...] = v
+
+
+def all_w(f):
+    return [getattr(f, n) for n in NAMES]
+
+
+@pytest.mark.parametrize("kvn", [False, True])
+@pytest.mark.parametrize("fast", [False, True])
+def test_elementwise_and_transforms(kvn, fast):
+    p = small(16, kvn, fast)
+    f, o = pair(p, kvn)
+    set_state(f, o)
+    f.Fourier_X_To_Lambda_64_64_4x4_GPU(*all_w(f))
+    for W in o.W:
+        o.x_to_lambda(W)
+    assert err16(comps(f), o.W) < 1e-12
+    f.ParticleProjector_GPU(*all_w(f), 1)
+    o.projector(o.W, 1)
+    assert err16(comps(f), o.W) < 1e-12
+    f.exp_p_lambda_GPU(*all_w(f))
+    o.kinetic(o.W)
+    assert err16(comps(f), o.W) < 1e-12
+    for which, fn in ((1, o.lambda_to_x), (2, o.p_to_theta)):
+        f._transform(all_w(f), which)
+        for W in o.W:
+            fn(W)
+    assert err16(comps(f), o.W) < 1e-12
+    f.Potential_Propagator(*all_w(f))
+    o.potential(o.W)
+    assert err16(comps(f), o.W) < 1e-12
+    f.Fourier_Theta_To_P_64_64_4x4_GPU(*all_w(f))
+    for W in o.W:
+        o.theta_to_p(W)
+    assert err16(comps(f), o.W) < 1e-12
+    f.boundary_xp_GPU(*all_w(f), 0.005, 15.0)
+    o.boundary_xp(o.W, 0.005, 15.0)
+    for k in (0, 5, 10, 15):
+        f.Real_GPU(getattr(f, NAMES[k]))
+        o.real(o.W[k])
+    assert err16(comps(f), o.W) < 1e-12
+    ob = o.observables(o.W)
+    got = f._reduce()
+    for name, k in [("average_x", 2), ("average_p_x_square", 5), ("average_Alpha_1", 10),
+                    ("average_Alpha_2_y", 13), ("energyKinetic", 14), ("energyPotential", 15),
+                    ("average_D_1_A_0", 16), ("average_D_1_A_2", 18)]:
+        assert abs(got[k] - ob[name]) <= 1e-12 * max(1.0, abs(ob[name])), name
+
+
+@pytest.mark.parametrize("kvn", [False, True])
+def test_initial_states(kvn):
+    p = small(16, kvn)
+    f, o = pair(p, kvn)
+    Ws = all_w(f)
+    f.WignerDiracGaussian_ParticleUp_GPU(*Ws, 0.5, 0.1, 0.3, -0.2, 2.2, 1.9)
+    o.particle_up(0.5, 0.1, 0.3, -0.2, 2.2, 1.9)
+    assert err16(comps(f), o.W) < 1e-14
+    f.WignerDiracGaussian_Majorana_GPU(*Ws, 0.5, 0.1, 0.3, -0.2, 2.2, 1.9, 1)
+    o.majorana(0.5, 0.1, 0.3, -0.2, 2.2, 1.9)
+    assert err16(comps(f), o.W) < 1e-14
+    f.WignerLandaoGround_GPU(*Ws, 0.26, 0.0, 0.0)
+    o.landau_ground(0.26)
+    assert err16(comps(f), o.W) < 1e-14
+
+
+@pytest.mark.parametrize("kvn,fast,alias,filt", [(False, False, True, False), (False, True, False, True),
+                                                  (True, False, True, True), (True, True, False, False)])
+def test_run_parity(kvn, fast, alias, filt):
+    p = small(16, kvn, fast)
+    f, o = pair(p, kvn, alias_w21=alias, FilterParticle=filt, bound_p=15.0)
+    set_state(f, o, 3)
+    f.timeSteps = 3
+    f.fileName = None
+    f.Run()
+    Ws = o.pointers(alias)
+    norms, obs = [], []
+    for _ in range(4):
+        n, ob = o.run_iteration(Ws, filter_particle=filt, bound_p=15.0)
+        norms.append(n)
+        obs.append(ob)
+    assert rel_err(f.norms, np.array(norms)) < 1e-12
+    for name in ["average_x", "average_p_y", "energyKinetic", "energyPotential", "average_Alpha_1"]:
+        assert rel_err(getattr(f, name), np.array([ob[name] for ob in obs])) < 1e-11, name
+    assert err16(comps(f), o.W) < 1e-11
+
+
+def test_golden_x_notebook_on_gpu():
+    """instances/WignerDirac4D_64_64/X.ipynb: init norm 9065.39215134, then the
+    Run() norms 0.9999809946, 10.3216821369, 10.321709756 (mask constant 7)."""
+    name = "instances/WignerDirac4D_64_64/X.ipynb"
+    cfg = NOTEBOOKS[name]
+    f = make_frame(GPU_WignerDirac4D, cfg["params"], bound_p=7.0)
+    Ws = all_w(f)
+    f.WignerDiracGaussian_ParticleUp_GPU(*Ws, 0.5, 0.0, 0.0, 0.0, 2.2, 2.2)
+    f._Fourier_Theta_To_P_64_64_4x4_GPU(*Ws)
+    f.boundary_p_GPU(*Ws)
+    for k in (0, 5, 10, 15):
+        f.Real_GPU(Ws[k])
+    n0 = f.Normalize_4x4_GPU(*Ws)
+    g = GOLD[name]
+    assert abs(n0.real - g["init_norms"][0]) < 1e-11 * g["init_norms"][0]
+    f.timeSteps = 2
+    f.fileName = None
+    f.Run()
+    for k in range(3):
+        assert abs(f.norms[k].real - g["run_norms"][k]) < 1e-10 * g["run_norms"][k], k
