@@ -173,6 +173,29 @@ int wig4d_init_gaussian(wig4d_plan* plan, void* W, double mu_p_y, double mu_y,
                         double mu_p_x, double mu_x, double s_p_y, double s_y,
                         double s_p_x, double s_x, void* stream);
 
+/*
+ * Observables of a state without any device allocation.  This entry point
+ * has no counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc (a fixed memory pool, a footprint budget, pre-registered
+ * buffers only) and therefore cannot create a plan either: it computes what
+ * wig4d_reduce computes -- d_out[2 * WIG4D_NOBS], the Run()-style row then
+ * the raw row -- from device tables the caller already holds: the four axis
+ * coordinate vectors, K(p_x, p_y) on [N_py][N_px] and V(x, y) on [N_y][N_x]
+ * (see wig4d_desc).  Its partial sums live in a fixed array inside the
+ * library (WIG4D_NOALLOC_MAX_COLUMNS * 12 doubles, 1.5 MiB, held by every GPU
+ * that loads the library until the process exits); grids with
+ * N_y * N_x > WIG4D_NOALLOC_MAX_COLUMNS return WIG_ERR_TOO_LARGE.  The first
+ * call on a device looks up the array's device address, so make it before
+ * any stream capture.  All calls share the array: calls whose kernels
+ * overlap on the GPU race; calls ordered on one stream do not.
+ */
+#define WIG4D_NOALLOC_MAX_COLUMNS 16384
+int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
+                              const double* d_coord_py, const double* d_coord_y,
+                              const double* d_coord_px, const double* d_coord_x,
+                              const double* d_energy_p, const double* d_energy_x,
+                              double dv_norm, double dv_obs, double* d_out, void* stream);
+
 /* Bytes of device memory the plan holds (tables, partial sums). */
 long long wig4d_plan_device_bytes(const wig4d_plan* plan);
 

@@ -54,6 +54,8 @@ __device__ __forceinline__ double2 zinv(double2 a) {
 // error is kept per host thread for wig_last_error().
 // ---------------------------------------------------------------------------
 void wig_set_cuda_error(cudaError_t e, const char* where);
+// the per-thread buffer wig_last_error() returns (256 bytes)
+char* wig_last_error_buffer();
 
 #define WIG_CUDA(call)                                                      \
     do {                                                                    \

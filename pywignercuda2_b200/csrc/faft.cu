@@ -39,6 +39,8 @@ int wig_num_sms() {
 
 extern "C" const char* wig_last_error(void) { return g_last_err; }
 
+char* wig_last_error_buffer() { return g_last_err; }
+
 extern "C" const char* wig_status_string(int s) {
     switch (s) {
         case WIG_OK: return "ok";

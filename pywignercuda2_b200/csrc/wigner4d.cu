@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -1185,6 +1186,89 @@ extern "C" int wig4d_reduce(wig4d_plan* p, const void* W, double* d_out, void* s
                                  : reduce_impl<float2>(p, (const float2*)W, st);
     if (s) return s;
     return finalize(p, d_out, nullptr, 0, st, d_out + WIG4D_NOBS);
+}
+
+// ---------------------------------------------------------------------------
+// Observables without any device allocation.
+//
+// Some callers cannot allocate device memory: code running where cudaMalloc
+// is not allowed or not wanted (an application with its own fixed memory
+// pool or a memory budget that forbids the library from growing its
+// footprint, or a host that only hands out pre-registered buffers).  They
+// also cannot create a plan, since wig4d_plan_create allocates its tables.
+// wig4d_observables_noalloc computes what wig4d_reduce computes from tables
+// the caller already holds on the device, and keeps its per-column partial
+// sums in the fixed array below instead of plan memory.
+//
+// The array is part of the library image: every GPU that loads the library
+// holds it (WIG4D_NOALLOC_MAX_COLUMNS * NPART doubles, 1.5 MiB) until the
+// process exits.  All calls share it, so two calls whose kernels overlap on
+// the GPU (different streams, or different host threads on one device) race
+// on it; calls on one stream are ordered and safe.  Every partial a call
+// reads is first written by the same call, so nothing needs clearing.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_noalloc_partials[(size_t)WIG4D_NOALLOC_MAX_COLUMNS * NPART];
+
+// Device address of g_noalloc_partials, looked up once per device with the
+// device current (in host code the symbol is only a stand-in, not an address).
+static double* noalloc_scratch(int* status) {
+    static std::mutex mu;
+    static double* addr[64] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) { wig_set_cuda_error(e, "cudaGetDevice"); *status = WIG_ERR_CUDA; return nullptr; }
+    if (dev < 0 || dev >= 64) { *status = WIG_ERR_UNSUPPORTED; return nullptr; }
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void* ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_noalloc_partials);
+        if (e != cudaSuccess || !ptr) {
+            wig_set_cuda_error(e, "cudaGetSymbolAddress(g_noalloc_partials)");
+            *status = WIG_ERR_CUDA;
+            return nullptr;
+        }
+        addr[dev] = static_cast<double*>(ptr);
+    }
+    *status = WIG_OK;
+    return addr[dev];
+}
+
+extern "C" int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
+                                         const double* d_coord_py, const double* d_coord_y,
+                                         const double* d_coord_px, const double* d_coord_x,
+                                         const double* d_energy_p, const double* d_energy_x,
+                                         double dv_norm, double dv_obs, double* d_out, void* stream) {
+    if (!W || !shape || !d_coord_py || !d_coord_y || !d_coord_px || !d_coord_x || !d_energy_p ||
+        !d_energy_x || !d_out)
+        return WIG_ERR_INVALID_ARG;
+    if (dtype != WIG_C128 && dtype != WIG_C64) return WIG_ERR_INVALID_ARG;
+    for (int a = 0; a < 4; ++a)
+        if (shape[a] < 1) return WIG_ERR_INVALID_ARG;
+    const long long columns = (long long)shape[1] * shape[3];
+    if (columns > WIG4D_NOALLOC_MAX_COLUMNS) {
+        snprintf(wig_last_error_buffer(), 256,
+                 "wig4d_observables_noalloc: N_y * N_x = %lld is above the fixed limit %d", columns,
+                 WIG4D_NOALLOC_MAX_COLUMNS);
+        return WIG_ERR_TOO_LARGE;
+    }
+    int status = WIG_OK;
+    double* partials = noalloc_scratch(&status);
+    if (!partials) return status;
+    ObsTabs ob;
+    ob.cpy = d_coord_py; ob.cy = d_coord_y; ob.cpx = d_coord_px; ob.cx = d_coord_x;
+    ob.ep = d_energy_p; ob.ex = d_energy_x;
+    cudaStream_t st = as_stream(stream);
+    if (dtype == WIG_C128)
+        k_reduce_xp<double2, 256><<<(unsigned)columns, 256, 0, st>>>((const double2*)W, shape[0], shape[1],
+                                                                    shape[2], shape[3], ob, partials);
+    else
+        k_reduce_xp<float2, 256><<<(unsigned)columns, 256, 0, st>>>((const float2*)W, shape[0], shape[1],
+                                                                   shape[2], shape[3], ob, partials);
+    WIG_LAUNCHED("k_reduce_xp (noalloc)");
+    k_finalize<<<1, 1024, 0, st>>>(partials, (int)columns, shape[3], ob, dv_norm, dv_obs, d_out, nullptr, 0,
+                                   nullptr, nullptr, d_out + WIG4D_NOBS);
+    WIG_LAUNCHED("k_finalize (noalloc)");
+    return WIG_OK;
 }
 
 // One Run() iteration: kinetic (dividing by the current norm), potential
