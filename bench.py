@@ -83,11 +83,18 @@ def _peaks():
 
 
 def _traffic():
-    """DRAM bytes per launch from the committed ncu summary (profiles/)."""
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    from the committed ncu summary profiles/dram_traffic.txt: lines of
+    ``<kernel> <workload> <bytes>``."""
+    out = {}
     try:
-        return json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic.json")))
-    except (OSError, ValueError):
-        return {}
+        for ln in open(os.path.join(ROOT, "profiles", "dram_traffic.txt")):
+            f = ln.split()
+            if len(f) == 3 and not ln.startswith("#"):
+                out[(f[0], f[1])] = float(f[2])
+    except OSError:
+        pass
+    return out
 
 
 def _frame(dtype):
@@ -197,34 +204,26 @@ def main():
     hcheck = hist[:K].cpu().numpy()
     finite = bool(np.all(np.isfinite(hcheck)))
 
-    # ---- dominant-kernel roofline: each half-step kernel timed alone -------
+    # ---- dominant-kernel roofline ----------------------------------------------
+    # The same K iterations again, launched one by one with CUDA events around
+    # each kernel on the launching stream: average duration of each launch.
     P = int(np.prod(f.shape))
     state_bytes = P * 16
-    def time_kernel(fn, reps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        for _ in range(3):
-            fn(f.W_init_gpu)
-        torch.cuda.synchronize()
-        a.record(st)
-        for _ in range(reps):
-            fn(f.W_init_gpu)
-        b.record(st)
-        torch.cuda.synchronize()
-        return a.elapsed_time(b) / reps
-    kin_ms = time_kernel(f.kinetic_halfstep, 20)
-    pot_ms = time_kernel(f.potential_halfstep, 20)
-    dom_name, dom_ms = ("k_potential", pot_ms) if pot_ms >= kin_ms else ("k_kinetic", kin_ms)
+    kin_ms, pot_ms, fin_ms = [m / K for m in f.run_device_timed(f.W_init_gpu, K, hist)]
+    fast = f.shape == (64, 64, 64, 64)
+    names = ("k_half64<kin>", "k_half64<pot>") if fast else ("k_kinetic", "k_potential")
+    dom_name, dom_ms = (names[1], pot_ms) if pot_ms >= kin_ms else (names[0], kin_ms)
     peaks = _peaks()
     peak = peaks.get("hbm_gbs")
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
     alg_bytes = 2 * state_bytes            # one read + one write of the state per launch
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
-    tr = _traffic().get(dom_name + "_64^4_c128")
+    tr = _traffic().get((dom_name, "64x64x64x64_c128"))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": tr, "kernel": dom_name,
                 "peak_source": peak_src, "algorithmic_bytes_per_launch": alg_bytes,
-                "kinetic_ms": kin_ms, "potential_ms": pot_ms,
+                "kinetic_ms": kin_ms, "potential_ms": pot_ms, "finalize_ms": fin_ms,
                 "step_frac": (4 * state_bytes / (ms / K / 1e3) / 1e9) / peak}
 
     # ---- precision form (complex64) on the same workload ----------------------
@@ -269,7 +268,7 @@ def main():
             "grid_point_steps_per_s": value * P,
             "precision_form": {"dtype": "c64", "steps_per_s": K / (ms32 / 1e3),
                                "speedup_vs_plain": (K / (ms32 / 1e3)) / (K / (ms / 1e3))},
-            "gpu_launches": 3 * K, "finite": finite, "roofline": roofline, "clocks": clocks,
+            "gpu_launches": 3 * K + 3, "finite": finite, "roofline": roofline, "clocks": clocks,
             "e2e": {"value": ws * K / (e2e_ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d / K,
                     "d2h_bytes_per_step": d2h / K,
                     "note": "one Run() of K iterations: pinned H2D of the state, history and "

@@ -163,6 +163,16 @@ int wig4d_reduce(wig4d_plan* plan, const void* W, double* d_out, void* stream);
  * happens inside; the launches are replayed from a CUDA graph.
  */
 int wig4d_run(wig4d_plan* plan, void* W, int iterations, double* d_history, void* stream);
+/*
+ * wig4d_run with per-kernel timing (no counterpart in the reference): the
+ * same launches, issued one by one rather than from a graph, each iteration's
+ * kinetic half-step, potential half-step and finalize bracketed by CUDA
+ * events on `stream`.  ms_out (host, 3 doubles) receives the summed
+ * milliseconds of the three parts over all iterations.  Returns after the
+ * stream has finished the last iteration.
+ */
+int wig4d_run_timed(wig4d_plan* plan, void* W, int iterations, double* d_history, void* stream,
+                    double* ms_out);
 
 /* Initial states on the (x, p) grid, coordinates from desc.coord:
    HOscillatorGound_GPU (GPU_Wigner4D.py:233-245) and Gaussian_GPU (216-230). */

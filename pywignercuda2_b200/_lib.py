@@ -93,6 +93,7 @@ SIGNATURES = {
     "wig4d_apply_factor": [_P, _P, _I, _P],
     "wig4d_reduce": [_P, _P, _P, _P],
     "wig4d_run": [_P, _P, _I, _P, _P],
+    "wig4d_run_timed": [_P, _P, _I, _P, _P, _DP],
     "wig4d_init_ho_ground": [_P, _P, _D, _D, _D, _D, _D, _D, _D, _P],
     "wig4d_init_gaussian": [_P, _P, _D, _D, _D, _D, _D, _D, _D, _D, _P],
     "wig4d_plan_device_bytes": [_P],

@@ -1271,31 +1271,43 @@ extern "C" int wig4d_observables_noalloc(const void* W, const int shape[4], int 
     return WIG_OK;
 }
 
-// One Run() iteration: kinetic (dividing by the current norm), potential
-// with the partial sums of the new state, finalize into the history.
+// One Run() iteration in three parts: kinetic (dividing by the current norm),
+// potential with the partial sums of the new state, finalize into the history.
 template <class C>
-static int iteration(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t st) {
-    int s;
+static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t st, int part) {
     if (p->fast64) {
         constexpr size_t sm = sizeof(C) * (64 * lanes64::LD + 64 + 128 + 8 * lanes64::NT) + sizeof(double) * (12 * lanes64::NT + 16 + NSUM);
         C* T = reinterpret_cast<C*>(p->pingpong);
         const int nsm = wig_num_sms();
         const C* pvk = reinterpret_cast<const C*>(p->pv);
         const C* pvp = pvk + (size_t)p->shape[0] * p->shape[2] * 128;
-        k_half64<C, true><<<nsm, lanes64::NT, sm, st>>>(W, T, p->shape[0], p->shape[2], pvk,
-                                                        make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr);
-        WIG_LAUNCHED("k_half64<kin>");
-        k_half64<C, false><<<nsm, lanes64::NT, sm, st>>>(T, W, p->shape[1], p->shape[3], pvp,
-                                                         make_double2(p->pot_scale, 0.0), nullptr, p->ob, p->partials);
-        WIG_LAUNCHED("k_half64<pot>");
-        k_finalize_sums<<<1, 32 * NSUM, 0, st>>>(p->partials, nsm, p->dv_norm, p->dv_obs, hist, p->counter, rows,
-                                          p->cur_norm, p->flag);
-        WIG_LAUNCHED("k_finalize_sums");
+        if (part == 0) {
+            k_half64<C, true><<<nsm, lanes64::NT, sm, st>>>(W, T, p->shape[0], p->shape[2], pvk,
+                                                            make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr);
+            WIG_LAUNCHED("k_half64<kin>");
+        } else if (part == 1) {
+            k_half64<C, false><<<nsm, lanes64::NT, sm, st>>>(T, W, p->shape[1], p->shape[3], pvp,
+                                                             make_double2(p->pot_scale, 0.0), nullptr, p->ob, p->partials);
+            WIG_LAUNCHED("k_half64<pot>");
+        } else {
+            k_finalize_sums<<<1, 32 * NSUM, 0, st>>>(p->partials, nsm, p->dv_norm, p->dv_obs, hist, p->counter, rows,
+                                                     p->cur_norm, p->flag);
+            WIG_LAUNCHED("k_finalize_sums");
+        }
         return WIG_OK;
     }
-    if ((s = kinetic_impl<C>(p, W, p->cur_norm, st))) return s;
-    if ((s = potential_impl<C>(p, W, p->partials, st))) return s;
+    if (part == 0) return kinetic_impl<C>(p, W, p->cur_norm, st);
+    if (part == 1) return potential_impl<C>(p, W, p->partials, st);
     return finalize(p, hist, p->counter, rows, st);
+}
+
+template <class C>
+static int iteration(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t st) {
+    for (int part = 0; part < 3; ++part) {
+        int s = iteration_part<C>(p, W, hist, rows, st, part);
+        if (s) return s;
+    }
+    return WIG_OK;
 }
 
 template <class C>
@@ -1339,6 +1351,68 @@ extern "C" int wig4d_run(wig4d_plan* p, void* W, int iterations, double* d_histo
     cudaStream_t st = as_stream(stream);
     return p->dtype == WIG_C128 ? run_impl<double2>(p, (double2*)W, iterations, d_history, st)
                                 : run_impl<float2>(p, (float2*)W, iterations, d_history, st);
+}
+
+// Run() with the kernels of every iteration bracketed by CUDA events: the
+// same launches as run_impl, issued one by one instead of through the graph.
+// Events of up to RING iterations are in flight; a slot is read back (its
+// last event synchronised) before it is reused.
+template <class C>
+static int run_timed_impl(wig4d_plan* p, C* W, int iterations, double* hist, cudaStream_t st, double* ms) {
+    constexpr int RING = 64;
+    int s;
+    ms[0] = ms[1] = ms[2] = 0.0;
+    WIG_CUDA(cudaMemsetAsync(p->counter, 0, 2 * sizeof(int), st));
+    if ((s = reduce_impl<C>(p, W, st))) return s;
+    if ((s = finalize(p, hist, p->counter, iterations, st))) return s;
+    if (iterations <= 0) return WIG_OK;
+    cudaEvent_t ev[RING][4];
+    cudaEvent_t* flat = &ev[0][0];
+    int made = 0;
+    cudaError_t e = cudaSuccess;
+    while (made < RING * 4 && (e = cudaEventCreate(&flat[made])) == cudaSuccess) ++made;
+    if (e != cudaSuccess) {
+        for (int i = 0; i < made; ++i) cudaEventDestroy(flat[i]);
+        wig_set_cuda_error(e, "cudaEventCreate");
+        return WIG_ERR_CUDA;
+    }
+    auto collect = [&](int slot) -> cudaError_t {
+        cudaError_t r = cudaEventSynchronize(ev[slot][3]);
+        for (int k = 0; k < 3 && r == cudaSuccess; ++k) {
+            float t = 0.f;
+            r = cudaEventElapsedTime(&t, ev[slot][k], ev[slot][k + 1]);
+            ms[k] += t;
+        }
+        return r;
+    };
+    s = WIG_OK;
+    for (int i = 0; i < iterations && s == WIG_OK; ++i) {
+        const int slot = i % RING;
+        if (i >= RING && (e = collect(slot)) != cudaSuccess) { wig_set_cuda_error(e, "event readback"); s = WIG_ERR_CUDA; break; }
+        for (int part = 0; part < 3 && s == WIG_OK; ++part) {
+            if ((e = cudaEventRecord(ev[slot][part], st)) != cudaSuccess) { wig_set_cuda_error(e, "cudaEventRecord"); s = WIG_ERR_CUDA; break; }
+            s = iteration_part<C>(p, W, hist, iterations, st, part);
+        }
+        if (s == WIG_OK && (e = cudaEventRecord(ev[slot][3], st)) != cudaSuccess) {
+            wig_set_cuda_error(e, "cudaEventRecord"); s = WIG_ERR_CUDA;
+        }
+    }
+    if (s == WIG_OK) {
+        const int first = iterations > RING ? iterations - RING : 0;
+        for (int i = first; i < iterations && s == WIG_OK; ++i)
+            if ((e = collect(i % RING)) != cudaSuccess) { wig_set_cuda_error(e, "event readback"); s = WIG_ERR_CUDA; }
+    }
+    for (int i = 0; i < RING * 4; ++i) cudaEventDestroy(flat[i]);
+    if (s) return s;
+    return wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st);
+}
+
+extern "C" int wig4d_run_timed(wig4d_plan* p, void* W, int iterations, double* d_history, void* stream,
+                               double* ms_out) {
+    if (!p || !W || !d_history || !ms_out || iterations < 0) return WIG_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    return p->dtype == WIG_C128 ? run_timed_impl<double2>(p, (double2*)W, iterations, d_history, st, ms_out)
+                                : run_timed_impl<float2>(p, (float2*)W, iterations, d_history, st, ms_out);
 }
 
 extern "C" int wig4d_init_ho_ground(wig4d_plan* p, void* W, double x_mu, double y_mu, double px_mu,

@@ -312,6 +312,15 @@ class GPU_Wigner4D:
         _lib.call("wig4d_run", self._plan, self._check(W), int(iterations), history.data_ptr(),
                   stream_ptr())
 
+    def run_device_timed(self, W, iterations, history):
+        """run_device without the CUDA graph, each kernel bracketed by CUDA
+        events; returns the summed milliseconds of the kinetic half-steps,
+        potential half-steps and finalize kernels (synchronises)."""
+        ms = (ctypes.c_double * 3)()
+        _lib.call("wig4d_run_timed", self._plan, self._check(W), int(iterations), history.data_ptr(),
+                  stream_ptr(), ms)
+        return tuple(ms)
+
     def Run(self):
         iterations = self.timeSteps + 1
         W = self.W_init_gpu

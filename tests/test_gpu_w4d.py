@@ -223,3 +223,24 @@ def test_fast64_matches_generic_kernels(dtype, tol, monkeypatch):
     for name in OBS:
         assert rel_err(getattr(f1, name), getattr(f2, name)) < tol, name
     assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < (100 * tol if tol < 1e-6 else 10 * tol)
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_run_timed_matches_run(n):
+    """The event-bracketed Run() launches the same kernels as the graph."""
+    from configs import cat_xp
+    p, c = config2(1, n)
+    f = make_frame(GPU_Wigner4D, p)
+    W0 = cat_xp(f._coords, c)
+    iters = 70                      # more than the 64-slot event ring
+    h1 = torch.empty((iters, _lib.WIG4D_NOBS), dtype=torch.float64, device="cuda")
+    h2 = torch.empty_like(h1)
+    f.W_init_gpu.set(W0)
+    f.run_device(f.W_init_gpu, iters, h1)
+    W1 = f.W_init_gpu.get()
+    f.W_init_gpu.set(W0)
+    ms = f.run_device_timed(f.W_init_gpu, iters, h2)
+    W2 = f.W_init_gpu.get()
+    assert rel_err(h2.cpu().numpy(), h1.cpu().numpy()) < 1e-14
+    assert rel_err(W2, W1) < 1e-14
+    assert all(m > 0 for m in ms)
