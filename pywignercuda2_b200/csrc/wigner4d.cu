@@ -24,6 +24,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -659,6 +660,8 @@ __global__ void __launch_bounds__(32 * NSUM) k_finalize_sums(const double* __res
     }
 }
 
+#include "quad64.cuh"
+
 // Standalone reduction of a state in the (x, p) representation: same CTA
 // shape and partial layout as k_potential's epilogue.
 template <class C, int NT>
@@ -832,6 +835,7 @@ struct wig4d_plan {
     bool fast64;                   // 64^4 grid: Run() uses k_kin64 / k_pot64
     void* pingpong;                // second state buffer (layout [y][x][p_y][p_x])
     void* pv;                      // per-plane factor vectors of the two half-steps
+    bool quad64;                   // complex64 64^4 Run(): k_quad64 on the LA / LB layouts
     // CUDA graph of one Run() iteration, cached per (W, history, stream)
     cudaGraphExec_t graph;
     void* graph_W;
@@ -1113,12 +1117,46 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             k_plane_vectors<double2><<<(npl_p * 128 + 255) / 256, 256>>>(p->pot_d, 0, 2, 1, 3, p->shape[3], npl_p,
                                                                         pv + (size_t)npl_k * 128);
         } else {
-            cudaFuncSetAttribute(k_half64<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-            cudaFuncSetAttribute(k_half64<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-            float2* pv = (float2*)p->pv;
-            k_plane_vectors<float2><<<(npl_k * 128 + 255) / 256, 256>>>(p->kin_f, 1, 3, 0, 2, p->shape[2], npl_k, pv);
-            k_plane_vectors<float2><<<(npl_p * 128 + 255) / 256, 256>>>(p->pot_f, 0, 2, 1, 3, p->shape[3], npl_p,
-                                                                       pv + (size_t)npl_k * 128);
+            // complex64: k_quad64 takes FP64 plane vectors, built from FP64
+            // copies of the tables (the plan keeps only the float32 ones)
+            p->quad64 = true;
+            const int qsm = (int)quad64_smem_bytes();
+            cudaFuncSetAttribute(k_quad64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, qsm);
+            cudaFuncSetAttribute(k_quad64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, qsm);
+            cudaFree(p->pv);
+            p->pv = nullptr;
+            if (cudaMalloc(&p->pv, (size_t)(npl_k + npl_p) * 128 * sizeof(double2)) != cudaSuccess) {
+                free_plan(p); return WIG_ERR_ALLOC;
+            }
+            long long n64 = 0;
+            for (int i = 0; i < desc->n_kin; ++i) n64 += tab_elems(desc->kin[i]);
+            for (int i = 0; i < desc->n_pot; ++i) n64 += tab_elems(desc->pot[i]);
+            double2* t64 = nullptr;
+            if (n64 > 0 && cudaMalloc(&t64, (size_t)n64 * sizeof(double2)) != cudaSuccess) {
+                free_plan(p); return WIG_ERR_ALLOC;
+            }
+            FactorSet<double2> k64 = p->kin_d, p64 = p->pot_d;
+            long long o64 = 0;
+            bool ok = true;
+            for (int i = 0; i < desc->n_kin; ++i) {
+                const long long n = tab_elems(desc->kin[i]);
+                ok = ok && cudaMemcpy(t64 + o64, desc->kin[i].host_data, n * 16, cudaMemcpyHostToDevice) == cudaSuccess;
+                k64.data[i] = t64 + o64; o64 += n;
+            }
+            for (int i = 0; i < desc->n_pot; ++i) {
+                const long long n = tab_elems(desc->pot[i]);
+                ok = ok && cudaMemcpy(t64 + o64, desc->pot[i].host_data, n * 16, cudaMemcpyHostToDevice) == cudaSuccess;
+                p64.data[i] = t64 + o64; o64 += n;
+            }
+            double2* pv = (double2*)p->pv;
+            if (ok) {
+                k_plane_vectors<double2><<<(npl_k * 128 + 255) / 256, 256>>>(k64, 1, 3, 0, 2, p->shape[2], npl_k, pv);
+                k_plane_vectors<double2><<<(npl_p * 128 + 255) / 256, 256>>>(p64, 0, 2, 1, 3, p->shape[3], npl_p,
+                                                                            pv + (size_t)npl_k * 128);
+                ok = cudaDeviceSynchronize() == cudaSuccess;
+            }
+            cudaFree(t64);
+            if (!ok) { wig_set_cuda_error(cudaGetLastError(), "plane vectors"); free_plan(p); return WIG_ERR_CUDA; }
         }
         // the persistent kernels write one NSUM row per CTA
         if ((size_t)wig_num_sms() * NSUM > (size_t)p->shape[1] * p->shape[3] * NPART) {
@@ -1275,6 +1313,29 @@ extern "C" int wig4d_observables_noalloc(const void* W, const int shape[4], int 
 // potential with the partial sums of the new state, finalize into the history.
 template <class C>
 static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t st, int part) {
+    if constexpr (std::is_same<C, float2>::value) {
+        if (p->quad64) {
+            // W holds LB, the ping-pong buffer LA (converted around the loop)
+            float2* P = reinterpret_cast<float2*>(p->pingpong);
+            const double2* pv = reinterpret_cast<const double2*>(p->pv);
+            const int nsm = wig_num_sms();
+            constexpr size_t sm = quad64_smem_bytes();
+            if (part == 0) {
+                k_quad64<true><<<nsm, quad64::NT, sm, st>>>(P, W, p->shape[0], pv, make_double2(p->kin_scale, 0.0),
+                                                           p->cur_norm, p->ob, nullptr);
+                WIG_LAUNCHED("k_quad64<kin>");
+            } else if (part == 1) {
+                k_quad64<false><<<nsm, quad64::NT, sm, st>>>(W, P, p->shape[1], pv + (size_t)p->shape[0] * p->shape[2] * 128,
+                                                            make_double2(p->pot_scale, 0.0), nullptr, p->ob, p->partials);
+                WIG_LAUNCHED("k_quad64<pot>");
+            } else {
+                k_finalize_sums<<<1, 32 * NSUM, 0, st>>>(p->partials, nsm, p->dv_norm, p->dv_obs, hist, p->counter,
+                                                         rows, p->cur_norm, p->flag);
+                WIG_LAUNCHED("k_finalize_sums");
+            }
+            return WIG_OK;
+        }
+    }
     if (p->fast64) {
         constexpr size_t sm = sizeof(C) * (64 * lanes64::LD + 64 + 128 + 8 * lanes64::NT) + sizeof(double) * (12 * lanes64::NT + 16 + NSUM);
         C* T = reinterpret_cast<C*>(p->pingpong);
@@ -1310,6 +1371,25 @@ static int iteration(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t s
     return WIG_OK;
 }
 
+// Before the first iteration: the complex64 64^4 loop works on the LA / LB
+// layouts (the state moves to the ping-pong buffer as LA).
+static int enter_loop_layout(wig4d_plan* p, void* W, cudaStream_t st) {
+    if (!p->quad64) return WIG_OK;
+    k_to_quad_layout<<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)W, (float2*)p->pingpong, p->npts);
+    WIG_LAUNCHED("k_to_quad_layout");
+    return WIG_OK;
+}
+
+// After the last iteration: the state back in the reference layout, divided
+// by its norm (the final renormalisation, GPU_Wigner4D.py:516-517).
+static int leave_loop_layout(wig4d_plan* p, void* W, cudaStream_t st) {
+    if (!p->quad64) return wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st);
+    k_from_quad_layout<<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)p->pingpong, (float2*)W, p->npts,
+                                                          p->cur_norm);
+    WIG_LAUNCHED("k_from_quad_layout");
+    return WIG_OK;
+}
+
 template <class C>
 static int run_impl(wig4d_plan* p, C* W, int iterations, double* hist, cudaStream_t st) {
     int s;
@@ -1319,11 +1399,11 @@ static int run_impl(wig4d_plan* p, C* W, int iterations, double* hist, cudaStrea
     if ((s = reduce_impl<C>(p, W, st))) return s;
     if ((s = finalize(p, hist, p->counter, iterations, st))) return s;
     if (iterations <= 0) return WIG_OK;
+    if ((s = enter_loop_layout(p, W, st))) return s;
     // iteration 0 runs eagerly (kernel attributes get set outside any capture);
     // the rest replay a CUDA graph of one iteration
     if ((s = iteration<C>(p, W, hist, iterations, st))) return s;
-    if (iterations == 1)
-        return wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st);
+    if (iterations == 1) return leave_loop_layout(p, W, st);
     if (!p->graph || p->graph_W != (void*)W || p->graph_hist != hist || p->graph_rows != iterations) {
         if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
         cudaStream_t cap;
@@ -1342,8 +1422,7 @@ static int run_impl(wig4d_plan* p, C* W, int iterations, double* hist, cudaStrea
     }
     // iterations: the last row recorded is that of the final state
     for (int i = 1; i < iterations; ++i) WIG_CUDA(cudaGraphLaunch(p->graph, st));
-    // final renormalisation (GPU_Wigner4D.py:516-517)
-    return wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st);
+    return leave_loop_layout(p, W, st);
 }
 
 extern "C" int wig4d_run(wig4d_plan* p, void* W, int iterations, double* d_history, void* stream) {
@@ -1366,6 +1445,7 @@ static int run_timed_impl(wig4d_plan* p, C* W, int iterations, double* hist, cud
     if ((s = reduce_impl<C>(p, W, st))) return s;
     if ((s = finalize(p, hist, p->counter, iterations, st))) return s;
     if (iterations <= 0) return WIG_OK;
+    if ((s = enter_loop_layout(p, W, st))) return s;
     cudaEvent_t ev[RING][4];
     cudaEvent_t* flat = &ev[0][0];
     int made = 0;
@@ -1404,7 +1484,7 @@ static int run_timed_impl(wig4d_plan* p, C* W, int iterations, double* hist, cud
     }
     for (int i = 0; i < RING * 4; ++i) cudaEventDestroy(flat[i]);
     if (s) return s;
-    return wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st);
+    return leave_loop_layout(p, W, st);
 }
 
 extern "C" int wig4d_run_timed(wig4d_plan* p, void* W, int iterations, double* d_history, void* stream,

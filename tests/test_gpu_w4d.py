@@ -225,13 +225,13 @@ def test_fast64_matches_generic_kernels(dtype, tol, monkeypatch):
     assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < (100 * tol if tol < 1e-6 else 10 * tol)
 
 
-@pytest.mark.parametrize("n", [32, 64])
-def test_run_timed_matches_run(n):
+@pytest.mark.parametrize("n,dtype", [(32, np.complex128), (64, np.complex128), (64, np.complex64)])
+def test_run_timed_matches_run(n, dtype):
     """The event-bracketed Run() launches the same kernels as the graph."""
     from configs import cat_xp
     p, c = config2(1, n)
-    f = make_frame(GPU_Wigner4D, p)
-    W0 = cat_xp(f._coords, c)
+    f = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    W0 = cat_xp(f._coords, c).astype(dtype)
     iters = 70                      # more than the 64-slot event ring
     h1 = torch.empty((iters, _lib.WIG4D_NOBS), dtype=torch.float64, device="cuda")
     h2 = torch.empty_like(h1)
@@ -244,3 +244,21 @@ def test_run_timed_matches_run(n):
     assert rel_err(h2.cpu().numpy(), h1.cpu().numpy()) < 1e-14
     assert rel_err(W2, W1) < 1e-14
     assert all(m > 0 for m in ms)
+
+
+def test_run_quad64_c64_vs_oracle():
+    """complex64 at 64^4 runs k_quad64 on the LA / LB layouts; the state comes
+    back in the reference layout.  Float32 bar: 2e-5 relative after 3 steps."""
+    from configs import cat_xp
+    p, c = config2(2, 64)
+    f, o = _pair(p, np.complex64)
+    W0 = cat_xp(f._coords, c)
+    f.W_init_gpu.set(W0.astype(np.complex64))
+    f.timeSteps = 2
+    f.fileName = None
+    f.Run()
+    Wo, obs = o.run(W0.astype(np.complex64).astype(np.complex128), 2)
+    for name in OBS:
+        assert rel_err(getattr(f, name), obs[name]) < 2e-5, name
+    assert rel_err(f.norm, obs["norms"]) < 2e-5
+    assert rel_err(f.W_init_gpu.get(), Wo) < 2e-5
