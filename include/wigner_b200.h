@@ -174,6 +174,18 @@ int wig4d_run(wig4d_plan* plan, void* W, int iterations, double* d_history, void
 int wig4d_run_timed(wig4d_plan* plan, void* W, int iterations, double* d_history, void* stream,
                     double* ms_out);
 
+/*
+ * Batched Run() (no counterpart in the reference): n independent instances,
+ * each with its own plan, state (device, the plan's shape and dtype) and
+ * history (iterations rows of WIG4D_NOBS float64), advanced `iterations`
+ * Run() iterations together.  Every step is one CUDA graph launch whose
+ * branches are the instances' iterations, so instances of different sizes
+ * run concurrently.  Plans and states must be distinct (WIG_ERR_ALIAS).
+ * Each instance ends exactly as wig4d_run would leave it.
+ */
+int wig4d_run_batch(wig4d_plan* const* plans, void* const* states, int n, int iterations,
+                    double* const* d_histories, void* stream);
+
 /* Initial states on the (x, p) grid, coordinates from desc.coord:
    HOscillatorGound_GPU (GPU_Wigner4D.py:233-245) and Gaussian_GPU (216-230). */
 int wig4d_init_ho_ground(wig4d_plan* plan, void* W, double x_mu, double y_mu,
@@ -205,6 +217,12 @@ int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
                               const double* d_coord_px, const double* d_coord_x,
                               const double* d_energy_p, const double* d_energy_x,
                               double dv_norm, double dv_obs, double* d_out, void* stream);
+
+/* Which kernels a plan runs (no counterpart in the reference): info[0] fused
+   kinetic half-step, info[1] fused potential half-step, info[2] the 64^4
+   register-resident Run() kernels, info[3] the complex64 quad kernels; each
+   1 or 0. */
+int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
 
 /* Bytes of device memory the plan holds (tables, partial sums). */
 long long wig4d_plan_device_bytes(const wig4d_plan* plan);

@@ -10,8 +10,9 @@ reference-compatible Python classes that build its plans and call it.
 from ._lib import WignerError, load as load_library  # noqa: F401
 from .device import DeviceScalar, GPUArray  # noqa: F401
 from .wigner4d import GPU_Wigner4D  # noqa: F401
+from .batch import WignerBatch  # noqa: F401
 
 from .dirac4d import GPU_WignerDirac4D, GPU_WignerDiracKvN4D  # noqa: F401
 
-__all__ = ["GPU_Wigner4D", "GPU_WignerDirac4D", "GPU_WignerDiracKvN4D", "GPUArray", "DeviceScalar",
+__all__ = ["GPU_Wigner4D", "GPU_WignerDirac4D", "GPU_WignerDiracKvN4D", "WignerBatch", "GPUArray", "DeviceScalar",
            "WignerError", "load_library"]

@@ -94,6 +94,8 @@ SIGNATURES = {
     "wig4d_reduce": [_P, _P, _P, _P],
     "wig4d_run": [_P, _P, _I, _P, _P],
     "wig4d_run_timed": [_P, _P, _I, _P, _P, _DP],
+    "wig4d_plan_info": [_P, _IP],
+    "wig4d_run_batch": [_P, _P, _I, _I, _P, _P],
     "wig4d_init_ho_ground": [_P, _P, _D, _D, _D, _D, _D, _D, _D, _P],
     "wig4d_init_gaussian": [_P, _P, _D, _D, _D, _D, _D, _D, _D, _D, _P],
     "wig4d_plan_device_bytes": [_P],

@@ -73,3 +73,6 @@ static inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStre
 
 // Number of SMs of the current device (148 on B200), cached per process.
 int wig_num_sms();
+
+// Line lengths with a radix transform (Stockham passes of radix 8/4/3/2).
+static inline bool wig_radix_size(int n) { return n == 16 || n == 32 || n == 48 || n == 64 || n == 128; }

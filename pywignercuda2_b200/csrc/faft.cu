@@ -219,7 +219,7 @@ static int faft_impl(C* g, const int shape[4], int axis, double d, double delta,
     const int TL = 16;
     if (v.inner != 1 && v.inner % TL != 0) return WIG_ERR_UNSUPPORTED;
     if ((v.outer * v.inner) % TL != 0) return WIG_ERR_UNSUPPORTED;
-    const bool fast = (n == 16 || n == 32 || n == 64 || n == 128) && fabs(fabs(delta) * n - 1.0) < 1e-12;
+    const bool fast = wig_radix_size(n) && fabs(fabs(delta) * n - 1.0) < 1e-12;
     double sc = post * 2.0 * n * d;
     if (fast && (n / 2) % 2 == 1) sc = -sc;   // (-1)^(N/2)
     C scale = mk<C>((typename real_of<C>::type)sc, 0);
@@ -228,6 +228,7 @@ static int faft_impl(C* g, const int shape[4], int axis, double d, double delta,
         switch (n) {
             case 16: return fwd ? launch_fast<C, 16, true>(g, v, TL, scale, st) : launch_fast<C, 16, false>(g, v, TL, scale, st);
             case 32: return fwd ? launch_fast<C, 32, true>(g, v, TL, scale, st) : launch_fast<C, 32, false>(g, v, TL, scale, st);
+            case 48: return fwd ? launch_fast<C, 48, true>(g, v, TL, scale, st) : launch_fast<C, 48, false>(g, v, TL, scale, st);
             case 64: return fwd ? launch_fast<C, 64, true>(g, v, TL, scale, st) : launch_fast<C, 64, false>(g, v, TL, scale, st);
             default: return fwd ? launch_fast<C, 128, true>(g, v, TL, scale, st) : launch_fast<C, 128, false>(g, v, TL, scale, st);
         }

@@ -62,8 +62,20 @@ template <class C, bool FWD> __device__ __forceinline__ void dft8(C* v) {
     v[2] = cadd(e2, w2); v[6] = csub(e2, w2);
     v[3] = cadd(e3, w3); v[7] = csub(e3, w3);
 }
+// 3-point DFT: y1,2 = x0 - (x1 + x2)/2 -+ i (sqrt3/2)(x1 - x2) (FWD), signs of i swapped otherwise
+template <class C, bool FWD> __device__ __forceinline__ void dft3(C& v0, C& v1, C& v2) {
+    typedef typename real_of<C>::type R;
+    const R h = (R)0.86602540378443864676;
+    const C t1 = cadd(v1, v2), t2 = csub(v1, v2);
+    const C m = mk<C>(v0.x - (R)0.5 * t1.x, v0.y - (R)0.5 * t1.y);
+    const C s = FWD ? mk<C>(h * t2.y, -h * t2.x) : mk<C>(-h * t2.y, h * t2.x);   // -+ i h t2
+    v0 = cadd(v0, t1);
+    v1 = cadd(m, s);
+    v2 = csub(m, s);
+}
 template <class C, int R, bool FWD> __device__ __forceinline__ void dft_r(C* v) {
     if (R == 2) dft2<C, FWD>(v[0], v[1]);
+    else if (R == 3) dft3<C, FWD>(v[0], v[1], v[2]);
     else if (R == 4) dft4<C, FWD>(v[0], v[1], v[2], v[3]);
     else dft8<C, FWD>(v);
 }
@@ -92,7 +104,7 @@ __device__ __forceinline__ void stockham_pass(C* s, const LineMap& m, int Ns, co
                 const int step = N / (Ns * R);
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    C w = tw[(r * k * step) & (N - 1)];
+                    C w = tw[r * k * step];          // r k step < N
                     if (!FWD) w = cconj(w);
                     v[i][r] = cmul(v[i][r], w);
                 }
@@ -117,7 +129,7 @@ __device__ __forceinline__ void stockham_pass(C* s, const LineMap& m, int Ns, co
     __syncthreads();
 }
 
-// Full length-N transform of L lines (N in {16, 32, 64, 128}).
+// Full length-N transform of L lines (N in {16, 32, 48, 64, 128}).
 template <class C, int N, int L, int NT, bool FWD, bool LINE_FAST>
 __device__ __forceinline__ void fft_lines(C* s, const LineMap& m, const C* tw) {
     if (N == 16) {
@@ -126,6 +138,10 @@ __device__ __forceinline__ void fft_lines(C* s, const LineMap& m, const C* tw) {
     } else if (N == 32) {
         stockham_pass<C, N, 8, L, NT, FWD, LINE_FAST>(s, m, 1, tw);
         stockham_pass<C, N, 4, L, NT, FWD, LINE_FAST>(s, m, 8, tw);
+    } else if (N == 48) {
+        stockham_pass<C, N, 4, L, NT, FWD, LINE_FAST>(s, m, 1, tw);
+        stockham_pass<C, N, 4, L, NT, FWD, LINE_FAST>(s, m, 4, tw);
+        stockham_pass<C, N, 3, L, NT, FWD, LINE_FAST>(s, m, 16, tw);
     } else if (N == 64) {
         stockham_pass<C, N, 8, L, NT, FWD, LINE_FAST>(s, m, 1, tw);
         stockham_pass<C, N, 8, L, NT, FWD, LINE_FAST>(s, m, 8, tw);

@@ -843,7 +843,7 @@ struct wig4d_plan {
     int graph_rows;
 };
 
-static bool pow2_16_128(int n) { return n == 16 || n == 32 || n == 64 || n == 128; }
+static bool pow2_16_128(int n) { return wig_radix_size(n); }
 
 // Threads per CTA of the fused kernels: one radix-8 butterfly per thread and
 // pass for a 64 x 64 plane; smaller planes use fewer threads.
@@ -857,7 +857,7 @@ template <> FactorSet<double2>& pot_set<double2>(wig4d_plan* p) { return p->pot_
 template <> FactorSet<float2>& pot_set<float2>(wig4d_plan* p) { return p->pot_f; }
 
 // Dispatch a fused kernel over the supported plane sizes.
-#define WIG_PLANE_CASES(X) X(16, 16) X(32, 32) X(64, 64) X(128, 128) X(64, 128) X(128, 64)
+#define WIG_PLANE_CASES(X) X(16, 16) X(32, 32) X(48, 48) X(64, 64) X(128, 128) X(64, 128) X(128, 64)
 
 template <class C>
 static int launch_kinetic(wig4d_plan* p, C* W, const double* d_norm, cudaStream_t st) {
@@ -1179,6 +1179,12 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
     return WIG_OK;
 }
 
+extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
+    if (!p || !info) return WIG_ERR_INVALID_ARG;
+    info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64; info[3] = p->quad64;
+    return WIG_OK;
+}
+
 extern "C" long long wig4d_plan_device_bytes(const wig4d_plan* p) {
     if (!p) return -1;
     const long long N0 = p->shape[0], N1 = p->shape[1], N2 = p->shape[2], N3 = p->shape[3];
@@ -1430,6 +1436,78 @@ extern "C" int wig4d_run(wig4d_plan* p, void* W, int iterations, double* d_histo
     cudaStream_t st = as_stream(stream);
     return p->dtype == WIG_C128 ? run_impl<double2>(p, (double2*)W, iterations, d_history, st)
                                 : run_impl<float2>(p, (float2*)W, iterations, d_history, st);
+}
+
+// ---------------------------------------------------------------------------
+// Batched Run(): independent instances (own grid, dtype, factors, state and
+// history) advanced together.  Each instance's first iteration runs eagerly;
+// the others replay ONE CUDA graph per step whose branches are the
+// instances' iterations (a child graph each, no edges between them), so the
+// kernels of different instances run concurrently and a step costs one
+// graph launch.
+// ---------------------------------------------------------------------------
+static int batch_prologue(wig4d_plan* p, void* W, double* hist, int iterations, cudaStream_t st) {
+    int s;
+    WIG_CUDA(cudaMemsetAsync(p->counter, 0, 2 * sizeof(int), st));
+    if (p->dtype == WIG_C128) {
+        if ((s = reduce_impl<double2>(p, (const double2*)W, st))) return s;
+    } else {
+        if ((s = reduce_impl<float2>(p, (const float2*)W, st))) return s;
+    }
+    if ((s = finalize(p, hist, p->counter, iterations, st))) return s;
+    if (iterations <= 0) return WIG_OK;
+    if ((s = enter_loop_layout(p, W, st))) return s;
+    return p->dtype == WIG_C128 ? iteration<double2>(p, (double2*)W, hist, iterations, st)
+                                : iteration<float2>(p, (float2*)W, hist, iterations, st);
+}
+
+extern "C" int wig4d_run_batch(wig4d_plan* const* plans, void* const* states, int n, int iterations,
+                               double* const* d_histories, void* stream) {
+    if (!plans || !states || !d_histories || n < 0 || iterations < 0) return WIG_ERR_INVALID_ARG;
+    for (int i = 0; i < n; ++i) {
+        if (!plans[i] || !states[i] || !d_histories[i]) return WIG_ERR_INVALID_ARG;
+        for (int j = 0; j < i; ++j)
+            if (plans[j] == plans[i] || states[j] == states[i]) return WIG_ERR_ALIAS;
+    }
+    cudaStream_t st = as_stream(stream);
+    int s;
+    for (int i = 0; i < n; ++i)
+        if ((s = batch_prologue(plans[i], states[i], d_histories[i], iterations, st))) return s;
+    if (iterations > 1 && n > 0) {
+        cudaGraph_t parent = nullptr;
+        WIG_CUDA(cudaGraphCreate(&parent, 0));
+        cudaStream_t cap = nullptr;
+        cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+        s = WIG_OK;
+        for (int i = 0; i < n && e == cudaSuccess && s == WIG_OK; ++i) {
+            wig4d_plan* p = plans[i];
+            cudaGraph_t child = nullptr;
+            e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) break;
+            s = p->dtype == WIG_C128 ? iteration<double2>(p, (double2*)states[i], d_histories[i], iterations, cap)
+                                     : iteration<float2>(p, (float2*)states[i], d_histories[i], iterations, cap);
+            const cudaError_t e2 = cudaStreamEndCapture(cap, &child);
+            if (s == WIG_OK) e = e2;
+            if (child) {
+                cudaGraphNode_t node;
+                if (s == WIG_OK && e == cudaSuccess) e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
+                cudaGraphDestroy(child);
+            }
+        }
+        if (cap) cudaStreamDestroy(cap);
+        cudaGraphExec_t exec = nullptr;
+        if (s == WIG_OK && e == cudaSuccess) e = cudaGraphInstantiate(&exec, parent, 0);
+        cudaGraphDestroy(parent);
+        if (s) return s;
+        if (e != cudaSuccess) { wig_set_cuda_error(e, "batch graph"); return WIG_ERR_CUDA; }
+        for (int it = 1; it < iterations && e == cudaSuccess; ++it) e = cudaGraphLaunch(exec, st);
+        cudaGraphExecDestroy(exec);      // deferred by the driver until the launches finish
+        if (e != cudaSuccess) { wig_set_cuda_error(e, "cudaGraphLaunch"); return WIG_ERR_CUDA; }
+    }
+    if (iterations > 0)
+        for (int i = 0; i < n; ++i)
+            if ((s = leave_loop_layout(plans[i], states[i], st))) return s;
+    return WIG_OK;
 }
 
 // Run() with the kernels of every iteration bracketed by CUDA events: the

@@ -296,6 +296,16 @@ class GPU_Wigner4D:
     def exp_x_theta_GPU(self, W):
         _lib.call("wig4d_apply_factor", self._plan, self._check(W), 1, stream_ptr())
 
+    def plan_info(self):
+        """Kernels the plan runs: fused_kinetic, fused_potential, fast64, quad64."""
+        info = (ctypes.c_int * 4)()
+        _lib.call("wig4d_plan_info", self._plan, info)
+        return dict(zip(("fused_kinetic", "fused_potential", "fast64", "quad64"), (bool(v) for v in info)))
+
+    def _plan_fused(self):
+        i = self.plan_info()
+        return i["fused_kinetic"], i["fused_potential"]
+
     # ---- fused half-steps ---------------------------------------------------------
     def kinetic_halfstep(self, W):
         """Fourier_X_To_Lambda + exp_p_lambda_GPU + Fourier_Lambda_To_X in one kernel."""
@@ -326,7 +336,11 @@ class GPU_Wigner4D:
         W = self.W_init_gpu
         hist = torch.empty((max(iterations, 1), _lib.WIG4D_NOBS), dtype=torch.float64, device="cuda")
         self.run_device(W, iterations, hist)
-        h = hist.cpu().numpy()[:iterations]
+        self._store_history(hist.cpu().numpy()[:iterations])
+
+    def _store_history(self, h):
+        """Run()'s result attributes (and the Ehrenfest file) from the history rows."""
+        iterations = h.shape[0]
         if not np.all(np.isfinite(h)):
             raise FloatingPointError("Run(): non-finite norm or observable")
         self.norm = h[:, 0] + 1j * h[:, 1]

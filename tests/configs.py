@@ -63,3 +63,18 @@ def cat_xp(coords, c, sep=1.5):
     g = lambda dx, dy: np.exp(-(x - x0 - dx) ** 2 - (px - px0) ** 2 - (y - y0 - dy) ** 2 - (py - py0) ** 2)
     w = g(sep, 0.0) + g(-sep, 0.0) + 2 * g(0.0, 0.0) * np.cos(2 * sep * (px - px0))
     return (w / np.pi ** 2).astype(np.complex128)
+
+
+def config4(seed=0, sizes=(32,) * 16 + (48,) * 16 + (64,) * 16):
+    """The batched workload: one instance per entry of ``sizes``, each with its
+    own quartic / coupling coefficients, Gaussian centre, D ~ U[0.001, 0.02]
+    and dt in {0.005, 0.01}.  Returns [(params, centre), ...]."""
+    rng = np.random.default_rng(seed + 4000)
+    out = []
+    for i, n in enumerate(sizes):
+        q = float(rng.uniform(0.05, 0.2))
+        kappa = float(rng.uniform(0.0, 0.1))
+        D = float(rng.uniform(0.001, 0.02))
+        dt = float(rng.choice([0.005, 0.01]))
+        out.append((w4d_params(n, q=q, kappa=kappa, D=D, dt=dt), centres(seed * 1000 + i)))
+    return out

@@ -30,7 +30,7 @@ def _rand(shape, seed, dtype=np.complex128):
 
 
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
-@pytest.mark.parametrize("shape", [(16, 16, 32, 32), (32, 16, 16, 64), (16, 32, 16, 16)])
+@pytest.mark.parametrize("shape", [(16, 16, 32, 32), (32, 16, 16, 64), (16, 32, 16, 16), (48, 16, 48, 16)])
 @pytest.mark.parametrize("axis", [0, 1, 2, 3])
 @pytest.mark.parametrize("dn", [1.0, -1.0, 0.7, -0.83])
 def test_faft_kernel(dtype, shape, axis, dn):
@@ -262,3 +262,15 @@ def test_run_quad64_c64_vs_oracle():
         assert rel_err(getattr(f, name), obs[name]) < 2e-5, name
     assert rel_err(f.norm, obs["norms"]) < 2e-5
     assert rel_err(f.W_init_gpu.get(), Wo) < 2e-5
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-12), (np.complex64, 1e-4)])
+def test_run_48_radix3_parity(dtype, tol):
+    """48 = 3 x 16 points per axis: fused half-steps with a radix-3 pass."""
+    p, c = config1(5, 48)
+    init = lambda f, o: o.ho_ground(c[0], c[1], c[2], c[3], 1.0, 1.0, 1.0) / np.pi ** 2
+    f, Wo, obs = _run_both(p, init, 6, dtype)
+    assert f._plan_fused() == (True, True)
+    for name in OBS:
+        assert rel_err(getattr(f, name), obs[name]) < tol, name
+    assert rel_err(f.W_init_gpu.get(), Wo) < (1e-10 if tol < 1e-6 else 1e-3)
