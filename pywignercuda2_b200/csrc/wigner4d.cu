@@ -275,6 +275,120 @@ __global__ void __launch_bounds__(NT, PlaneCfg<NPY, NPX, NT>::MINB) k_potential(
 }
 
 // ---------------------------------------------------------------------------
+// Fused potential half-step over G neighbouring (y, x) columns per CTA.
+//
+// A (p_y, p_x) plane at fixed (y, x) is a gather at stride N_x; taking the
+// planes x0 .. x0+G-1 together makes every access a run of G elements
+// (G * 16 or G * 8 = 64 bytes), and cp.async moves them straight into shared
+// memory.  There are no centring sign flips: with S = (-1)^(p_x + p_y),
+// S IFFT2(F FFT2(S w)) = IFFT2(F' FFT2(w)), F'[k] = F[k + N/2], so the factor
+// is read at frequencies shifted by N/2.  One partial row per column, as
+// k_potential writes.
+// ---------------------------------------------------------------------------
+template <class C, int NPY, int NPX, int G>
+struct PotCfg {
+    static constexpr int NT = 256;
+    static constexpr int LD = NPX + 1;                              // row stride
+    static constexpr int PSP = ((NPY * LD + 13) / 16) * 16 + 2;     // plane stride, = 2 (mod 16)
+    static constexpr int PTS = NPY * NPX;
+    static constexpr size_t bytes() {
+        return sizeof(C) * ((size_t)G * PSP + NPX + NPY) + sizeof(double) * NPART * (NT / 32);
+    }
+};
+
+__device__ __forceinline__ void cp_async_elem(double2* dst, const double2* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(float2* dst, const float2* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <class C, int NPY, int NPX, int G>
+__global__ void __launch_bounds__(256, 1) k_potential_g(C* __restrict__ W, int ny, int nx, FactorSet<C> F,
+                                                        double2 scale, ObsTabs ob, double* __restrict__ partials) {
+    typedef PotCfg<C, NPY, NPX, G> P;
+    constexpr int NT = P::NT;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* s = reinterpret_cast<C*>(smraw);
+    C* twx = s + G * P::PSP;
+    C* twy = twx + NPX;
+    double* red = reinterpret_cast<double*>(twy + NPY);
+    const int nxg = nx / G;
+    const int x0 = (blockIdx.x % nxg) * G, iy = blockIdx.x / nxg;
+    make_twiddles(twx, NPX);
+    if (NPY != NPX) make_twiddles(twy, NPY);
+    const C* ty = (NPY != NPX) ? twy : twx;
+    const long long pys = (long long)ny * NPX * nx;     // stride of p_y
+    C* gb = W + (long long)iy * NPX * nx + x0;          // element (p_y, p_x, g): gb[p_y*pys + p_x*nx + g]
+    for (int e = threadIdx.x; e < G * P::PTS; e += NT) {
+        const int g = e % G, px = (e / G) % NPX, py = e / (G * NPX);
+        cp_async_elem(s + g * P::PSP + py * P::LD + px, gb + py * pys + (long long)px * nx + g);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // the planes' transforms one after another (registers as for one plane)
+    const LineMap rows{1, P::LD, 0, 1}, cols{1, 1, 0, P::LD};
+    for (int g = 0; g < G; ++g) {
+        fft_lines<C, NPX, NPY, NT, true, true>(s + g * P::PSP, rows, twx);
+        fft_lines<C, NPY, NPX, NT, true, true>(s + g * P::PSP, cols, ty);
+    }
+    const C cc = to_c<C>(scale);
+    for (int e = threadIdx.x; e < G * P::PTS; e += NT) {
+        const int g = e / P::PTS, r = e % P::PTS, py = r / NPX, px = r % NPX;
+        const int ky = (py + NPY / 2) % NPY, kx = (px + NPX / 2) % NPX, ix = x0 + g;
+        const long long lin = ky * pys + (long long)iy * NPX * nx + (long long)kx * nx + ix;
+        C* q = s + g * P::PSP + py * P::LD + px;
+        *q = cmul(*q, factor_at(F, ky, iy, kx, ix, lin, cc));
+    }
+    __syncthreads();
+    for (int g = 0; g < G; ++g) {
+        fft_lines<C, NPY, NPX, NT, false, true>(s + g * P::PSP, cols, ty);
+        fft_lines<C, NPX, NPY, NT, false, true>(s + g * P::PSP, rows, twx);
+    }
+    for (int e = threadIdx.x; e < G * P::PTS; e += NT) {
+        const int g = e % G, px = (e / G) % NPX, py = e / (G * NPX);
+        gb[py * pys + (long long)px * nx + g] = s[g * P::PSP + py * P::LD + px];
+    }
+    if (partials) {
+        // plane-major: NT / G threads per column, in whole warps
+        constexpr int TPP = NT / G;
+        const int g = threadIdx.x / TPP, t = threadIdx.x % TPP;
+        double a[NPART];
+#pragma unroll
+        for (int i = 0; i < NPART; ++i) a[i] = 0.0;
+        for (int r = t; r < P::PTS; r += TPP) {
+            const int py = r / NPX, px = r % NPX;
+            const double2 w = to_d2(s[g * P::PSP + py * P::LD + px]);
+            const double qx = __ldg(ob.cpx + px), qy = __ldg(ob.cpy + py), k = __ldg(ob.ep + py * NPX + px);
+            a[0] += w.x; a[1] += w.y;
+            a[2] = fma(qx, w.x, a[2]); a[3] = fma(qx, w.y, a[3]);
+            a[4] = fma(qx * qx, w.x, a[4]); a[5] = fma(qx * qx, w.y, a[5]);
+            a[6] = fma(qy, w.x, a[6]); a[7] = fma(qy, w.y, a[7]);
+            a[8] = fma(qy * qy, w.x, a[8]); a[9] = fma(qy * qy, w.y, a[9]);
+            a[10] = fma(k, w.x, a[10]); a[11] = fma(k, w.y, a[11]);
+        }
+#pragma unroll
+        for (int i = 0; i < NPART; ++i)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) a[i] += __shfl_down_sync(0xffffffffu, a[i], o);
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        if (l == 0)
+#pragma unroll
+            for (int i = 0; i < NPART; ++i) red[w * NPART + i] = a[i];
+        __syncthreads();
+        if (threadIdx.x < G * NPART) {
+            const int gg = threadIdx.x / NPART, i = threadIdx.x % NPART;
+            double sum = 0.0;
+            for (int k = 0; k < TPP / 32; ++k) sum += red[(gg * (TPP / 32) + k) * NPART + i];
+            partials[((long long)iy * nx + x0 + gg) * NPART + i] = sum;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Run() kernels for 64 x 64 x 64 x 64 grids: register-resident transforms
 // (lanes64.cuh) and a ping-pong layout between the two half-steps.
 //
@@ -880,6 +994,31 @@ static int launch_kinetic(wig4d_plan* p, C* W, const double* d_norm, cudaStream_
     return WIG_ERR_UNSUPPORTED;
 }
 
+// The G-column potential kernel, when G columns fit in shared memory and N_x
+// is a multiple of G (G = 4 for complex128, 8 for complex64, halved until the
+// CTA fits).  Returns false when it does not apply.
+template <class C, int NPY, int NPX, int G>
+static bool launch_potential_gn(wig4d_plan* p, C* W, double* partials, cudaStream_t st, double2 sc) {
+    if constexpr (G < 2) {
+        return false;
+    } else {
+        typedef PotCfg<C, NPY, NPX, G> P;
+        if (P::bytes() > 227 * 1024 || p->shape[3] % G != 0)
+            return launch_potential_gn<C, NPY, NPX, G / 2>(p, W, partials, st, sc);
+        auto kern = k_potential_g<C, NPY, NPX, G>;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::bytes()) != cudaSuccess)
+            return false;
+        const unsigned grid = (unsigned)(p->shape[1] * (p->shape[3] / G));
+        kern<<<grid, P::NT, P::bytes(), st>>>(W, p->shape[1], p->shape[3], pot_set<C>(p), sc, p->ob, partials);
+        return cudaGetLastError() == cudaSuccess;
+    }
+}
+template <class C, int NPY, int NPX>
+static bool launch_potential_g(wig4d_plan* p, C* W, double* partials, cudaStream_t st, double2 sc) {
+    if (getenv("WIG_NO_POT_G")) return false;
+    return launch_potential_gn<C, NPY, NPX, (sizeof(C) == 16 ? 4 : 8)>(p, W, partials, st, sc);
+}
+
 template <class C>
 static int launch_potential(wig4d_plan* p, C* W, double* partials, cudaStream_t st) {
     const int NPY = p->shape[0], NPX = p->shape[2];
@@ -888,6 +1027,7 @@ static int launch_potential(wig4d_plan* p, C* W, double* partials, cudaStream_t 
     const double2 sc = make_double2(p->pot_scale, 0.0);
 #define PCASE(a, b)                                                                      \
     if (NPY == a && NPX == b) {                                                          \
+        if (launch_potential_g<C, a, b>(p, W, partials, st, sc)) return WIG_OK;           \
         constexpr int NT = FusedNT<a, b>::v;                                             \
         auto kern = k_potential<C, a, b, NT>;                                            \
         size_t sm = plane_bytes<C, a, b>();                                              \
