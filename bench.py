@@ -131,6 +131,55 @@ def cpu_baseline_port(steps, workers, budget_s=20.0):
     return n / dt, n, dt
 
 
+def bench_batched(steps):
+    """The batched workload: 48 instances (16 each at 32^4, 48^4, 64^4, own
+    coefficients, centres, D and dt) advanced together in complex64 through
+    WignerBatch, against the same 48 run one at a time in the plain complex128
+    form.  Aggregate grid-point steps per second, CUDA events."""
+    import torch
+    from configs import config4, gaussian_xp
+    from frames import make_frame
+    from pywignercuda2_b200 import GPU_Wigner4D, WignerBatch
+    cfg = config4(0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    frames = []
+    for params, c in cfg:
+        f = make_frame(GPU_Wigner4D, dict(params, timeSteps=steps - 1), complex_dtype=np.complex64)
+        f.W_init_gpu.set(gaussian_xp(f._coords, c).astype(np.complex64))
+        frames.append(f)
+    pts = sum(int(np.prod(f.shape)) for f in frames)
+    batch = WignerBatch(frames)
+    hists = [torch.empty((steps, 11), dtype=torch.float64, device="cuda") for _ in frames]
+    batch.run_device(3, hists)
+    torch.cuda.synchronize()
+    e0.record()
+    batch.run_device(steps, hists)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_batch = e0.elapsed_time(e1)
+    finite = all(bool(torch.isfinite(h).all()) for h in hists)
+    del batch, frames, hists
+    ms_plain = 0.0
+    for params, c in cfg:
+        f = make_frame(GPU_Wigner4D, dict(params, timeSteps=steps - 1))
+        f.W_init_gpu.set(gaussian_xp(f._coords, c))
+        h = torch.empty((steps, 11), dtype=torch.float64, device="cuda")
+        f.run_device(f.W_init_gpu, 3, h)
+        torch.cuda.synchronize()
+        e0.record()
+        f.run_device(f.W_init_gpu, steps, h)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_plain += e0.elapsed_time(e1)
+        del f, h
+    return {"workload": "48 instances: 16 x 32^4, 16 x 48^4, 16 x 64^4, seeded q, kappa, centre, "
+                        "D in U[0.001, 0.02], dt in {0.005, 0.01}", "steps": steps,
+            "grid_points": pts, "dtype": "c64",
+            "gp_steps_per_s": pts * steps / (ms_batch / 1e3), "ms": ms_batch, "finite": finite,
+            "one_at_a_time_plain_c128": {"gp_steps_per_s": pts * steps / (ms_plain / 1e3), "ms": ms_plain},
+            "speedup_vs_one_at_a_time_plain": ms_plain / ms_batch}
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -158,6 +207,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched 48-instance line")
+    ap.add_argument("--batch-steps", type=int, default=100)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -306,6 +357,8 @@ def main():
                     "d2h_bytes_per_step": d2h / K,
                     "note": "one Run() of K iterations: pinned H2D of the state, history and "
                             "final state read back"}}
+    if not args.no_batch:
+        line["batched_form"] = bench_batched(args.batch_steps)
     if rank == 0 and not args.no_cpu_baseline:
         v, n, dt = cpu_baseline_port(3, workers=1, budget_s=20.0)
         line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": 1, "kind": "port",
