@@ -180,6 +180,61 @@ def bench_batched(steps):
             "speedup_vs_one_at_a_time_plain": ms_plain / ms_batch}
 
 
+def bench_dirac(steps):
+    """The Wigner-Dirac workload: 64^4 grid x 16 components (4.3 GB in
+    complex128), V = 0.3 (x^2 + y^2), symmetric-gauge field B in U[0.1, 0.5],
+    D_lambda = 0.005, dt = 0.002, delta = 1/N windows, positive-energy Gaussian
+    spinor.  Steps/s of Run() in the reference's call sequence (the W21 alias,
+    the default) and of the fused device loop (alias off), CUDA events."""
+    import math
+    import torch
+    from frames import make_frame
+    from pywignercuda2_b200 import GPU_WignerDirac4D
+    from pywignercuda2_b200.dirac4d import NAMES
+    rng = np.random.default_rng(5000)
+    B = float(rng.uniform(0.1, 0.5))
+    x0, y0 = (float(v) for v in rng.uniform(-2, 2, size=2))
+    n, amp_x, amp_p = 64, 8.0, 8.0
+    dx, dp = 2 * amp_x / n, 2 * amp_p / n
+    params = dict(gridDIM_p_y=n, gridDIM_y=n, gridDIM_p_x=n, gridDIM_x=n, dt=0.002, timeSteps=steps - 1,
+                  p_y_amplitude=amp_p, y_amplitude=amp_x, p_x_amplitude=amp_p, x_amplitude=amp_x,
+                  theta_y_amplitude=math.pi / dp, theta_x_amplitude=math.pi / dp,
+                  lambda_y_amplitude=math.pi / dx, lambda_x_amplitude=math.pi / dx,
+                  c=1.0, HBar=1.0, mass=1.0, potential_0_String="0.3*(x*x + y*y)",
+                  potential_1_String="-%r*y/2." % B, potential_2_String="%r*x/2." % B,
+                  potential_3_String="0.", D_1_potential_0_String="0.6*x", D_1_potential_1_String="0.",
+                  D_1_potential_2_String="%r/2." % B, D_theta_x=0.0, D_theta_y=0.0,
+                  D_lambda_x=0.005, D_lambda_y=0.005)
+    out = {"workload": "WignerDirac4D 64^4 x 16 components, complex128, B=%.3f, dt=0.002" % B,
+           "state_bytes": 16 * n ** 4 * 16, "steps": steps}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f = make_frame(GPU_WignerDirac4D, params)
+    f.fileName = None
+    Ws = [getattr(f, k) for k in NAMES]
+    for alias in (True, False):
+        f.alias_w21 = alias
+        def init():                            # the notebooks' preparation: (x, theta) -> (x, p)
+            f.WignerDiracGaussian_ParticleUp_GPU(*Ws, 0.0, 0.0, x0, y0, 1.0, 1.0)
+            f._Fourier_Theta_To_P_64_64_4x4_GPU(*Ws)
+        init()
+        f.timeSteps = 1
+        f.Run()                                # warm-up (plans, graphs)
+        init()
+        f.timeSteps = steps - 1
+        torch.cuda.synchronize()
+        e0.record()
+        f.Run()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        key = "reference_sequence" if alias else "fused_loop"
+        out[key] = {"steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps,
+                    "hbm_gbs_per_sweep_equivalent": 2 * out["state_bytes"] / (ms / steps / 1e3) / 1e9,
+                    "finite": bool(np.all(np.isfinite(f.energyKinetic)))}
+    del f
+    return out
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -209,6 +264,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 48-instance line")
     ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--no-dirac", action="store_true", help="skip the Wigner-Dirac line")
+    ap.add_argument("--dirac-steps", type=int, default=20)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -359,6 +416,8 @@ def main():
                             "final state read back"}}
     if not args.no_batch:
         line["batched_form"] = bench_batched(args.batch_steps)
+    if not args.no_dirac:
+        line["dirac_form"] = bench_dirac(args.dirac_steps)
     if rank == 0 and not args.no_cpu_baseline:
         v, n, dt = cpu_baseline_port(3, workers=1, budget_s=20.0)
         line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": 1, "kind": "port",

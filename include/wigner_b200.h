@@ -164,6 +164,16 @@ int wig4d_reduce(wig4d_plan* plan, const void* W, double* d_out, void* stream);
  */
 int wig4d_run(wig4d_plan* plan, void* W, int iterations, double* d_history, void* stream);
 /*
+ * wig4d_run with flags (no counterpart in the reference).  WIG_RUN_KEEP_NORM
+ * skips the final renormalisation, so that consecutive calls continue one
+ * Run() exactly: the next call's first history row is the norm the skipped
+ * division would have used, and its first step divides by it.  Run() with
+ * snapshots is split this way.
+ */
+#define WIG_RUN_KEEP_NORM 1
+int wig4d_run_ex(wig4d_plan* plan, void* W, int iterations, double* d_history, int flags, void* stream);
+
+/*
  * wig4d_run with per-kernel timing (no counterpart in the reference): the
  * same launches, issued one by one rather than from a graph, each iteration's
  * kinetic half-step, potential half-step and finalize bracketed by CUDA

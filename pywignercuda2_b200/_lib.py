@@ -11,6 +11,7 @@ LIB_PATH = os.path.join(HERE, "libwigner_b200.so")
 
 WIG_MAX_FACTORS = 12
 WIG4D_NOBS = 11
+WIG_RUN_KEEP_NORM = 1
 C128, C64 = 0, 1
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported shape or parameter", 3: "CUDA error",
@@ -93,6 +94,7 @@ SIGNATURES = {
     "wig4d_apply_factor": [_P, _P, _I, _P],
     "wig4d_reduce": [_P, _P, _P, _P],
     "wig4d_run": [_P, _P, _I, _P, _P],
+    "wig4d_run_ex": [_P, _P, _I, _P, _I, _P],
     "wig4d_run_timed": [_P, _P, _I, _P, _P, _DP],
     "wig4d_plan_info": [_P, _IP],
     "wig4d_run_batch": [_P, _P, _I, _I, _P, _P],

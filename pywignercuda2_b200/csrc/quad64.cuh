@@ -346,10 +346,11 @@ __global__ void k_to_quad_layout(const float2* __restrict__ W, float2* __restric
     }
 }
 
-// LA -> L0 with the final division by the complex norm; one thread per L0 element.
+// LA -> L0 with the final division by the complex norm (none when d_norm is
+// null); one thread per L0 element.
 __global__ void k_from_quad_layout(const float2* __restrict__ P, float2* __restrict__ W, long long n,
                                    const double* __restrict__ d_norm) {
-    const double2 inv = zinv(make_double2(d_norm[0], d_norm[1]));
+    const double2 inv = d_norm ? zinv(make_double2(d_norm[0], d_norm[1])) : make_double2(1.0, 0.0);
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
         const int x = (int)(e & 63), px = (int)((e >> 6) & 63), y = (int)((e >> 12) & 63), py = (int)(e >> 18);
         const float2 a = P[((((long long)y * 16 + (x >> 2)) * 64 + py) * 64 + px) * 4 + (x & 3)];

@@ -1528,16 +1528,16 @@ static int enter_loop_layout(wig4d_plan* p, void* W, cudaStream_t st) {
 
 // After the last iteration: the state back in the reference layout, divided
 // by its norm (the final renormalisation, GPU_Wigner4D.py:516-517).
-static int leave_loop_layout(wig4d_plan* p, void* W, cudaStream_t st) {
-    if (!p->quad64) return wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st);
+static int leave_loop_layout(wig4d_plan* p, void* W, cudaStream_t st, bool divide = true) {
+    if (!p->quad64) return divide ? wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st) : WIG_OK;
     k_from_quad_layout<<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)p->pingpong, (float2*)W, p->npts,
-                                                          p->cur_norm);
+                                                          divide ? p->cur_norm : nullptr);
     WIG_LAUNCHED("k_from_quad_layout");
     return WIG_OK;
 }
 
 template <class C>
-static int run_impl(wig4d_plan* p, C* W, int iterations, double* hist, cudaStream_t st) {
+static int run_impl(wig4d_plan* p, C* W, int iterations, double* hist, cudaStream_t st, bool divide = true) {
     int s;
     // counter = 0, flag = 0
     WIG_CUDA(cudaMemsetAsync(p->counter, 0, 2 * sizeof(int), st));
@@ -1549,7 +1549,7 @@ static int run_impl(wig4d_plan* p, C* W, int iterations, double* hist, cudaStrea
     // iteration 0 runs eagerly (kernel attributes get set outside any capture);
     // the rest replay a CUDA graph of one iteration
     if ((s = iteration<C>(p, W, hist, iterations, st))) return s;
-    if (iterations == 1) return leave_loop_layout(p, W, st);
+    if (iterations == 1) return leave_loop_layout(p, W, st, divide);
     if (!p->graph || p->graph_W != (void*)W || p->graph_hist != hist || p->graph_rows != iterations) {
         if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
         cudaStream_t cap;
@@ -1568,14 +1568,19 @@ static int run_impl(wig4d_plan* p, C* W, int iterations, double* hist, cudaStrea
     }
     // iterations: the last row recorded is that of the final state
     for (int i = 1; i < iterations; ++i) WIG_CUDA(cudaGraphLaunch(p->graph, st));
-    return leave_loop_layout(p, W, st);
+    return leave_loop_layout(p, W, st, divide);
+}
+
+extern "C" int wig4d_run_ex(wig4d_plan* p, void* W, int iterations, double* d_history, int flags, void* stream) {
+    if (!p || !W || !d_history || iterations < 0 || (flags & ~WIG_RUN_KEEP_NORM)) return WIG_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    const bool divide = !(flags & WIG_RUN_KEEP_NORM);
+    return p->dtype == WIG_C128 ? run_impl<double2>(p, (double2*)W, iterations, d_history, st, divide)
+                                : run_impl<float2>(p, (float2*)W, iterations, d_history, st, divide);
 }
 
 extern "C" int wig4d_run(wig4d_plan* p, void* W, int iterations, double* d_history, void* stream) {
-    if (!p || !W || !d_history || iterations < 0) return WIG_ERR_INVALID_ARG;
-    cudaStream_t st = as_stream(stream);
-    return p->dtype == WIG_C128 ? run_impl<double2>(p, (double2*)W, iterations, d_history, st)
-                                : run_impl<float2>(p, (float2*)W, iterations, d_history, st);
+    return wig4d_run_ex(p, W, iterations, d_history, 0, stream);
 }
 
 // ---------------------------------------------------------------------------

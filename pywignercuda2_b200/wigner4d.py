@@ -20,6 +20,14 @@ Extra attributes a frame may set (defaults reproduce the reference):
   built in float64 and rounded once, float64 reductions).
 * ``round_constants``: True reproduces the reference's '%f' formatting of the
   device constants (GPU_Wigner4D.py:128-150); False uses full precision.
+* ``snapshotEvery``: K > 0 makes Run() keep the normalised state every K
+  iterations in ``self.snapshots`` (list of (time, array)) and write them
+  beside the Ehrenfest data (``/Snapshots/W_<i>``); the observables and the
+  final state are those of a Run() without snapshots.
+
+``save_checkpoint(fname)`` / ``load_checkpoint(fname)`` store and restore the
+state so that a later Run() continues the run (no counterpart in the
+reference).
 """
 import ctypes
 import os
@@ -334,9 +342,67 @@ class GPU_Wigner4D:
     def Run(self):
         iterations = self.timeSteps + 1
         W = self.W_init_gpu
-        hist = torch.empty((max(iterations, 1), _lib.WIG4D_NOBS), dtype=torch.float64, device="cuda")
-        self.run_device(W, iterations, hist)
-        self._store_history(hist.cpu().numpy()[:iterations])
+        every = int(getattr(self, "snapshotEvery", 0) or 0)
+        if every <= 0 or every >= iterations:
+            hist = torch.empty((max(iterations, 1), _lib.WIG4D_NOBS), dtype=torch.float64, device="cuda")
+            self.run_device(W, iterations, hist)
+            self._store_history(hist.cpu().numpy()[:iterations])
+            return
+        # Snapshots: the loop runs in chunks of `every` iterations; between
+        # chunks the final renormalisation is skipped (WIG_RUN_KEEP_NORM), so
+        # the chunks continue one Run().  Snapshot t is the state whose
+        # observables row t records, normalised as Run() normalises it.
+        rows, self.snapshots = [], []
+        self._W0_copy = W.get()
+        t = 0
+        while t < iterations:
+            n = min(every, iterations - t)
+            last = t + n >= iterations
+            hist = torch.empty((n, _lib.WIG4D_NOBS), dtype=torch.float64, device="cuda")
+            _lib.call("wig4d_run_ex", self._plan, self._check(W), n, hist.data_ptr(),
+                      0 if last else _lib.WIG_RUN_KEEP_NORM, stream_ptr())
+            h = hist.cpu().numpy()
+            # the state that entered this chunk, normalised by its row-0 norm
+            self.snapshots.append((t * self.dt, self._snapshot_from(self._W0_copy, h[0])))
+            rows.append(h)
+            t += n
+            if not last:
+                self._W0_copy = W.get()
+        self._store_history(np.concatenate(rows)[:iterations])
+        self._write_snapshots()
+
+    def _snapshot_from(self, Wh, row):
+        return Wh / complex(row[0], row[1])
+
+    def _write_snapshots(self):
+        fname = getattr(self, "fileName", None)
+        if fname and self.snapshots:
+            write_snapshots(fname, self.snapshots)
+
+    # ---- checkpoint / resume (no counterpart in the reference) -----------------
+    def save_checkpoint(self, fname):
+        """Save the current state and the result attributes of the last Run()
+        to ``fname`` (.npz).  A frame built with the same attributes continues
+        the run after ``load_checkpoint``: its Run() starts from this state."""
+        data = {"W": self.W_init_gpu.get(), "shape": np.array(self.shape),
+                "dt": np.array(self.dt), "time_offset": np.array(self._time_offset_next())}
+        for k in RESULT_NAMES:
+            if hasattr(self, k):
+                data[k] = np.asarray(getattr(self, k))
+        np.savez(fname, **data)
+
+    def load_checkpoint(self, fname):
+        """Restore a state saved by ``save_checkpoint`` into ``W_init_gpu``."""
+        with np.load(fname) as z:
+            if tuple(z["shape"]) != self.shape:
+                raise ValueError("checkpoint grid %s != %s" % (tuple(z["shape"]), self.shape))
+            self.W_init_gpu.set(z["W"].astype(self.W_init_gpu.dtype))
+            self.time_offset = float(z["time_offset"])
+
+    def _time_offset_next(self):
+        # the state after the last Run() is len(energy) steps past its start
+        t0 = float(getattr(self, "time_offset", 0.0))
+        return t0 + len(getattr(self, "energy", ())) * self.dt
 
     def _store_history(self, h):
         """Run()'s result attributes (and the Ehrenfest file) from the history rows."""
@@ -349,7 +415,7 @@ class GPU_Wigner4D:
         self.average_y, self.average_p_y = h[:, 6], h[:, 7]
         self.average_y_square, self.average_p_y_square = h[:, 8], h[:, 9]
         self.energy = h[:, 10]
-        self.timeRange = np.arange(iterations) * self.dt
+        self.timeRange = float(getattr(self, "time_offset", 0.0)) + np.arange(iterations) * self.dt
         fname = getattr(self, "fileName", None)
         if fname:
             write_ehrenfest(fname, {
@@ -359,6 +425,27 @@ class GPU_Wigner4D:
                 "average_p_x_square": self.average_p_x_square,
                 "average_y_square": self.average_y_square,
                 "average_p_y_square": self.average_p_y_square})
+
+
+RESULT_NAMES = ("norm", "average_x", "average_p_x", "average_x_square", "average_p_x_square", "average_y",
+                "average_p_y", "average_y_square", "average_p_y_square", "energy", "timeRange")
+
+
+def write_snapshots(fname, snaps):
+    """Run()'s snapshots as ``/Snapshots/W_<i>`` with ``/Snapshots/time``:
+    added to the HDF5 file when h5py is importable, else written to
+    ``<fileName>.snapshots.npz`` with keys ``time`` and ``W_<i>``."""
+    times = np.array([t for t, _ in snaps])
+    try:
+        import h5py
+    except ImportError:
+        np.savez(fname + ".snapshots.npz", time=times, **{"W_%d" % i: w for i, (_, w) in enumerate(snaps)})
+        return fname + ".snapshots.npz"
+    with h5py.File(fname, "a") as f:
+        f["/Snapshots/time"] = times
+        for i, (_, w) in enumerate(snaps):
+            f["/Snapshots/W_%d" % i] = w
+    return fname
 
 
 def write_ehrenfest(fname, data):
