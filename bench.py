@@ -353,8 +353,10 @@ def main():
     P = int(np.prod(f.shape))
     state_bytes = P * 16
     kin_ms, pot_ms, fin_ms = [m / K for m in f.run_device_timed(f.W_init_gpu, K, hist)]
-    fast = f.shape == (64, 64, 64, 64)
-    names = ("k_half64<kin>", "k_half64<pot>") if fast else ("k_kinetic", "k_potential")
+    run64 = f.plan_info()["run64_kernel"]
+    names = {"r4t": ("k_r4t<kin>", "k_r4t<pot>"), "r4": ("k_r4<kin>", "k_r4<pot>"),
+             "half64": ("k_half64<kin>", "k_half64<pot>")}.get(
+        run64, ("k_kinetic", "k_potential"))
     dom_name, dom_ms = (names[1], pot_ms) if pot_ms >= kin_ms else (names[0], kin_ms)
     peaks = _peaks()
     peak = peaks.get("hbm_gbs")
@@ -370,12 +372,13 @@ def main():
                 "step_frac": (4 * state_bytes / (ms / K / 1e3) / 1e9) / peak}
     k32, p32, _ = [m / K for m in f32.run_device_timed(f32.W_init_gpu, K, hist32)]
     d32 = max(k32, p32)
-    precision["roofline"] = {"bound": "hbm", "kernel": "k_quad64<pot>" if p32 >= k32 else "k_quad64<kin>",
+    kname = "k_r4" if f32.plan_info()["run64_kernel"] == "r4" else "k_quad64"
+    precision["roofline"] = {"bound": "hbm", "kernel": kname + ("<pot>" if p32 >= k32 else "<kin>"),
                              "achieved": state_bytes / (d32 / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                              "frac": state_bytes / (d32 / 1e3) / 1e9 / peak,
                              "algorithmic_bytes_per_launch": state_bytes,
                              "kinetic_ms": k32, "potential_ms": p32,
-                             "traffic": _traffic().get(("k_quad64<pot>" if p32 >= k32 else "k_quad64<kin>",
+                             "traffic": _traffic().get((kname + ("<pot>" if p32 >= k32 else "<kin>"),
                                                         "64x64x64x64_c64"))}
     del f32
 
@@ -409,7 +412,8 @@ def main():
                        "factor_mode": list(f._factor_mode)},
             "grid_point_steps_per_s": value * P,
             "precision_form": precision,
-            "gpu_launches": 3 * K + 3, "finite": finite, "roofline": roofline, "clocks": clocks,
+            "gpu_launches": (3 * K + 4) if run64 == "r4" else (3 * K + 3),
+            "finite": finite, "roofline": roofline, "clocks": clocks,
             "e2e": {"value": ws * K / (e2e_ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d / K,
                     "d2h_bytes_per_step": d2h / K,
                     "note": "one Run() of K iterations: pinned H2D of the state, history and "

@@ -55,7 +55,7 @@ def build(verbose=False, extra=()):
         objs = list(ex.map(lambda s: _compile(s, list(extra)), srcs))
     newest = max(os.path.getmtime(o) for o in objs)
     if not os.path.exists(OUT) or os.path.getmtime(OUT) < newest:
-        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart", "-lcuda"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), r.stderr))

@@ -20,12 +20,15 @@
 // The (-1)^n centring of the FAFT cancels between a forward and an inverse
 // transform of the same axis except on the plane's input and output, where
 // it is a sign flip; the 2 N d scales and wrapper divisors are one scalar.
+#include <cuda.h>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <type_traits>
 #include <vector>
+
+#include <cooperative_groups.h>
 
 #include "common.cuh"
 #include "fft_smem.cuh"
@@ -775,6 +778,7 @@ __global__ void __launch_bounds__(32 * NSUM) k_finalize_sums(const double* __res
 }
 
 #include "quad64.cuh"
+#include "r4.cuh"
 
 // Standalone reduction of a state in the (x, p) representation: same CTA
 // shape and partial layout as k_potential's epilogue.
@@ -842,13 +846,15 @@ __global__ void __launch_bounds__(1024) k_finalize(const double* __restrict__ pa
         for (int i = 0; i < NS; ++i) sm[w * NS + i] = a[i];
     }
     __syncthreads();
+    __shared__ double S[NS];
+    if (threadIdx.x < NS) {                          // one thread per sum, fixed order
+        double t = 0.0;
+#pragma unroll 8
+        for (int k = 0; k < 32; ++k) t += sm[k * NS + threadIdx.x];
+        S[threadIdx.x] = t;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        double S[NS];
-        for (int i = 0; i < NS; ++i) {
-            double t = 0.0;
-            for (int k = 0; k < 32; ++k) t += sm[k * NS + i];
-            S[i] = t;
-        }
         const double2 n = make_double2(S[0] * dv_norm, S[1] * dv_norm);
         const double2 inv = zinv(n);
         auto obs = [&](int k) { return dv_obs * (S[k] * inv.x - S[k + 1] * inv.y); };
@@ -950,6 +956,13 @@ struct wig4d_plan {
     void* pingpong;                // second state buffer (layout [y][x][p_y][p_x])
     void* pv;                      // per-plane factor vectors of the two half-steps
     bool quad64;                   // complex64 64^4 Run(): k_quad64 on the LA / LB layouts
+    bool r4;                       // 64^4 Run(): k_r4 (16 points per thread) on its LA / LB layouts
+    bool r4t;                      // complex128 64^4 Run(): k_r4 with TMA plane loads (k_r4t)
+    bool r4_cluster;               // k_r4 launched as clusters with full-sector stores
+    void* tw64;                    // k_r4 twiddle table (64 complex of the plan's dtype)
+    CUtensorMap map_t_load;        // LA view of the ping-pong buffer (kinetic source)
+    CUtensorMap map_w_load;        // LB view of the caller's state (potential source)
+    const void* map_w_ptr;                 // state the W maps describe
     // CUDA graph of one Run() iteration, cached per (W, history, stream)
     cudaGraphExec_t graph;
     void* graph_W;
@@ -1114,7 +1127,60 @@ static void free_plan(wig4d_plan* p) {
     cudaFree(p->cur_norm);
     cudaFree(p->pingpong);
     cudaFree(p->pv);
+    cudaFree(p->tw64);
     delete p;
+}
+
+// Tensor maps of a 64^4 complex128 array viewed as 4-D float64 [d3][d2][d1][d0]
+// with d0 = 128 (64 complex values): rows of 1 KB, planes of 64 KB.
+// cuTensorMapEncodeTiled through the runtime's driver entry point, so that the
+// library does not link the driver and still loads where no driver exists.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(f);
+    });
+    return fn;
+}
+
+// 5-D view of a 64^4 complex128 array in the LA / LB layouts of k_r4 (IL = 2):
+// (4 float64 = 2 points, f1, f0, c/2, r) with strides 32 B, 2 KB, 128 KB, 4 MB;
+// the box is one plane of either half-step.
+static int encode_plane_map(CUtensorMap* m, const void* base) {
+    const cuuint64_t dims[5] = {4, 64, 64, 32, 64};
+    const cuuint64_t strides[4] = {32, 2048, 128 * 1024, 4 * 1024 * 1024};
+    const cuuint32_t box[5] = {4, 1, 1, 32, 64};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    EncodeTiledFn enc = encode_tiled_fn();
+    if (!enc) {
+        snprintf(wig_last_error_buffer(), 256, "cuTensorMapEncodeTiled is not available from the driver");
+        return WIG_ERR_CUDA;
+    }
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<void*>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(wig_last_error_buffer(), 256, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return WIG_ERR_CUDA;
+    }
+    return WIG_OK;
+}
+
+// LB map of the caller's state W (the potential half-step's source).
+static int ensure_w_maps(wig4d_plan* p, const void* W) {
+    if (p->map_w_ptr == W) return WIG_OK;
+    int s;
+    if ((s = encode_plane_map(&p->map_w_load, W))) return s;
+    p->map_w_ptr = W;
+    return WIG_OK;
 }
 
 extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
@@ -1298,6 +1364,38 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             cudaFree(t64);
             if (!ok) { wig_set_cuda_error(cudaGetLastError(), "plane vectors"); free_plan(p); return WIG_ERR_CUDA; }
         }
+        // k_r4 with cluster stores (default); WIG_FAST64_KERNEL = r4 (plain
+        // stores), r4t (complex128 TMA loads) or pair (k_half64 / k_quad64)
+        const char* kern = getenv("WIG_FAST64_KERNEL");
+        p->r4 = !(kern && strcmp(kern, "pair") == 0);
+        if (p->r4 && desc->dtype == WIG_C128 && kern && strcmp(kern, "r4t") == 0) {
+            // k_r4 with TMA plane loads: LA map of the ping-pong buffer now,
+            // LB map of the caller's state at the first run
+            int r;
+            if ((r = encode_plane_map(&p->map_t_load, p->pingpong))) { free_plan(p); return r; }
+            p->r4t = true;
+            cudaFuncSetAttribute(k_r4t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4t_smem_bytes());
+            cudaFuncSetAttribute(k_r4t<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4t_smem_bytes());
+        }
+        if (p->r4) {
+            p->quad64 = false;
+            p->r4_cluster = !(kern && strcmp(kern, "r4") == 0);
+            if (cudaMalloc(&p->tw64, 64 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+            if (desc->dtype == WIG_C128) k_make_r4_twiddles<double2><<<1, 64>>>((double2*)p->tw64);
+            else k_make_r4_twiddles<float2><<<1, 64>>>((float2*)p->tw64);
+            const int rsm = (int)(desc->dtype == WIG_C128 ? r4_smem_bytes<double2>() : r4_smem_bytes<float2>());
+            if (desc->dtype == WIG_C128) {
+                cudaFuncSetAttribute(k_r4<double2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<double2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<double2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<double2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+            } else {
+                cudaFuncSetAttribute(k_r4<float2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<float2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<float2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<float2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+            }
+        }
         // the persistent kernels write one NSUM row per CTA
         if ((size_t)wig_num_sms() * NSUM > (size_t)p->shape[1] * p->shape[3] * NPART) {
             cudaFree(p->partials);
@@ -1321,7 +1419,8 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 
 extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     if (!p || !info) return WIG_ERR_INVALID_ARG;
-    info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64; info[3] = p->quad64;
+    info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64;
+    info[3] = !p->fast64 ? 0 : (p->r4t ? 4 : (p->r4 ? 3 : (p->quad64 ? 2 : 1)));
     return WIG_OK;
 }
 
@@ -1457,8 +1556,76 @@ extern "C" int wig4d_observables_noalloc(const void* W, const int shape[4], int 
 
 // One Run() iteration in three parts: kinetic (dividing by the current norm),
 // potential with the partial sums of the new state, finalize into the history.
+// k_r4 launch: with clusters of IL CTAs (full-sector stores) or plain.
+template <class C, bool KIN>
+static cudaError_t launch_r4(bool cluster, unsigned grid, size_t sm, cudaStream_t st, const C* src, C* dst,
+                             const double2* pv, const C* tw, double2 scale, const double* d_norm, ObsTabs ob,
+                             double* partials) {
+    if (!cluster) {
+        k_r4<C, KIN, false><<<grid, r4::NT, sm, st>>>(src, dst, pv, tw, scale, d_norm, ob, partials);
+        return cudaGetLastError();
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(r4::NT);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = r4::Il<C>::v;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_r4<C, KIN, true>, src, dst, pv, tw, scale, d_norm, ob, partials);
+}
+
 template <class C>
 static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t st, int part) {
+    if constexpr (std::is_same<C, double2>::value) {
+        if (p->r4t) {
+            int s;
+            if ((s = ensure_w_maps(p, W))) return s;
+            const double2* pv = reinterpret_cast<const double2*>(p->pv);
+            constexpr size_t sm = r4t_smem_bytes();
+            // kinetic: LA (ping-pong) -> LB (W); potential: LB (W) -> LA (ping-pong)
+            if (part == 0) {
+                k_r4t<true><<<64 * 64, r4::NT, sm, st>>>(p->map_t_load, W, pv, (const double2*)p->tw64,
+                                                         make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr);
+                WIG_LAUNCHED("k_r4t<kin>");
+            } else if (part == 1) {
+                k_r4t<false><<<64 * 64, r4::NT, sm, st>>>(p->map_w_load, reinterpret_cast<double2*>(p->pingpong),
+                                                          pv + (size_t)p->shape[0] * p->shape[2] * 128,
+                                                          (const double2*)p->tw64,
+                                                          make_double2(p->pot_scale, 0.0), p->cur_norm, p->ob,
+                                                          p->partials);
+                WIG_LAUNCHED("k_r4t<pot>");
+            } else {
+                return finalize(p, hist, p->counter, rows, st);
+            }
+            return WIG_OK;
+        }
+    }
+    if (p->r4) {
+        // W holds LB, the ping-pong buffer LA (converted around the loop)
+        C* P = reinterpret_cast<C*>(p->pingpong);
+        const double2* pv = reinterpret_cast<const double2*>(p->pv);
+        constexpr size_t sm = r4_smem_bytes<C>();
+        const unsigned nplanes = 64 * 64;
+        if (part == 0) {
+            WIG_CUDA((launch_r4<C, true>(p->r4_cluster, nplanes, sm, st, P, W, pv, (const C*)p->tw64,
+                                         make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr)));
+            WIG_LAUNCHED("k_r4<kin>");
+        } else if (part == 1) {
+            WIG_CUDA((launch_r4<C, false>(p->r4_cluster, nplanes, sm, st, W, P,
+                                          pv + (size_t)p->shape[0] * p->shape[2] * 128, (const C*)p->tw64,
+                                          make_double2(p->pot_scale, 0.0), nullptr, p->ob, p->partials)));
+            WIG_LAUNCHED("k_r4<pot>");
+        } else {
+            return finalize(p, hist, p->counter, rows, st);
+        }
+        return WIG_OK;
+    }
     if constexpr (std::is_same<C, float2>::value) {
         if (p->quad64) {
             // W holds LB, the ping-pong buffer LA (converted around the loop)
@@ -1520,6 +1687,14 @@ static int iteration(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t s
 // Before the first iteration: the complex64 64^4 loop works on the LA / LB
 // layouts (the state moves to the ping-pong buffer as LA).
 static int enter_loop_layout(wig4d_plan* p, void* W, cudaStream_t st) {
+    if (p->r4) {
+        if (p->dtype == WIG_C128)
+            k_to_r4_layout<double2><<<wig_num_sms() * 8, 256, 0, st>>>((const double2*)W, (double2*)p->pingpong, p->npts);
+        else
+            k_to_r4_layout<float2><<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)W, (float2*)p->pingpong, p->npts);
+        WIG_LAUNCHED("k_to_r4_layout");
+        return WIG_OK;
+    }
     if (!p->quad64) return WIG_OK;
     k_to_quad_layout<<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)W, (float2*)p->pingpong, p->npts);
     WIG_LAUNCHED("k_to_quad_layout");
@@ -1529,6 +1704,17 @@ static int enter_loop_layout(wig4d_plan* p, void* W, cudaStream_t st) {
 // After the last iteration: the state back in the reference layout, divided
 // by its norm (the final renormalisation, GPU_Wigner4D.py:516-517).
 static int leave_loop_layout(wig4d_plan* p, void* W, cudaStream_t st, bool divide = true) {
+    if (p->r4) {
+        const double* nrm = divide ? p->cur_norm : nullptr;
+        if (p->dtype == WIG_C128)
+            k_from_r4_layout<double2><<<wig_num_sms() * 8, 256, 0, st>>>((const double2*)p->pingpong, (double2*)W,
+                                                                         p->npts, nrm);
+        else
+            k_from_r4_layout<float2><<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)p->pingpong, (float2*)W,
+                                                                        p->npts, nrm);
+        WIG_LAUNCHED("k_from_r4_layout");
+        return WIG_OK;
+    }
     if (!p->quad64) return divide ? wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st) : WIG_OK;
     k_from_quad_layout<<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)p->pingpong, (float2*)W, p->npts,
                                                           divide ? p->cur_norm : nullptr);

@@ -305,10 +305,12 @@ class GPU_Wigner4D:
         _lib.call("wig4d_apply_factor", self._plan, self._check(W), 1, stream_ptr())
 
     def plan_info(self):
-        """Kernels the plan runs: fused_kinetic, fused_potential, fast64, quad64."""
+        """Kernels the plan runs: fused_kinetic, fused_potential, fast64, run64_kernel."""
         info = (ctypes.c_int * 4)()
         _lib.call("wig4d_plan_info", self._plan, info)
-        return dict(zip(("fused_kinetic", "fused_potential", "fast64", "quad64"), (bool(v) for v in info)))
+        run64 = {0: None, 1: "half64", 2: "quad64", 3: "r4", 4: "r4t"}[info[3]]
+        return {"fused_kinetic": bool(info[0]), "fused_potential": bool(info[1]), "fast64": bool(info[2]),
+                "run64_kernel": run64}
 
     def _plan_fused(self):
         i = self.plan_info()

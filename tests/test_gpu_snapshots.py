@@ -32,7 +32,10 @@ def _frame(n, dtype, steps, **kw):
 
 @pytest.mark.parametrize("n,dtype", [(32, np.complex128), (64, np.complex128), (64, np.complex64)])
 def test_snapshots_do_not_change_the_run(n, dtype):
-    tol = 1e-13 if dtype == np.complex128 else 1e-6
+    # complex64: the chunks' first steps divide by norms that differ in the
+    # last float32 places, which the float32 noise floor turns into 1e-6-level
+    # differences of the edge-weighted moments after a few steps
+    tol = 1e-13 if dtype == np.complex128 else 1e-4
     a, _ = _frame(n, dtype, 11)
     a.Run()
     b, W0 = _frame(n, dtype, 11, snapshotEvery=4)
@@ -46,7 +49,7 @@ def test_snapshots_do_not_change_the_run(n, dtype):
     # renormalises at the end, as the snapshot is normalised)
     c, _ = _frame(n, dtype, 3)
     c.Run()
-    assert rel_err(b.snapshots[1][1], c.W_init_gpu.get()) < (1e-12 if tol < 1e-6 else 1e-5)
+    assert rel_err(b.snapshots[1][1], c.W_init_gpu.get()) < (1e-12 if tol < 1e-6 else 1e-4)
     assert rel_err(b.snapshots[0][1], W0 / complex(a.norm[0])) < tol
 
 

@@ -274,3 +274,48 @@ def test_run_48_radix3_parity(dtype, tol):
     for name in OBS:
         assert rel_err(getattr(f, name), obs[name]) < tol, name
     assert rel_err(f.W_init_gpu.get(), Wo) < (1e-10 if tol < 1e-6 else 1e-3)
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-12), (np.complex64, 1e-4)])
+def test_r4_matches_pair_kernels(dtype, tol, monkeypatch):
+    """The default 64^4 kernels (k_r4 with cluster stores) against
+    k_half64 / k_quad64."""
+    from configs import cat_xp
+    p, c = config2(6, 64)
+    f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    monkeypatch.setenv("WIG_FAST64_KERNEL", "pair")
+    f2 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    monkeypatch.delenv("WIG_FAST64_KERNEL")
+    assert f1.plan_info()["run64_kernel"] == "r4"
+    assert f2.plan_info()["run64_kernel"] == ("half64" if dtype == np.complex128 else "quad64")
+    W0 = cat_xp(f1._coords, c).astype(dtype)
+    for f in (f1, f2):
+        f.W_init_gpu.set(W0)
+        f.timeSteps = 9
+        f.fileName = None
+        f.Run()
+    for name in OBS:
+        assert rel_err(getattr(f1, name), getattr(f2, name)) < tol, name
+    assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < (100 * tol if tol < 1e-6 else 10 * tol)
+
+
+@pytest.mark.parametrize("variant", ["r4t", "r4"])
+def test_r4_variants_match_default(variant, monkeypatch):
+    """complex128: k_r4 with TMA plane loads (r4t) and k_r4 with plain stores
+    (r4) against the default k_r4 with cluster stores: the same arithmetic."""
+    from configs import cat_xp
+    p, c = config2(7, 64)
+    f1 = make_frame(GPU_Wigner4D, p)
+    monkeypatch.setenv("WIG_FAST64_KERNEL", variant)
+    f2 = make_frame(GPU_Wigner4D, p)
+    monkeypatch.delenv("WIG_FAST64_KERNEL")
+    assert (f1.plan_info()["run64_kernel"], f2.plan_info()["run64_kernel"]) == ("r4", variant)
+    W0 = cat_xp(f1._coords, c)
+    for f in (f1, f2):
+        f.W_init_gpu.set(W0)
+        f.timeSteps = 9
+        f.fileName = None
+        f.Run()
+    for name in OBS:
+        assert rel_err(getattr(f1, name), getattr(f2, name)) < 1e-13, name
+    assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < 1e-12
