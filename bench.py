@@ -412,7 +412,7 @@ def main():
                        "factor_mode": list(f._factor_mode)},
             "grid_point_steps_per_s": value * P,
             "precision_form": precision,
-            "gpu_launches": (3 * K + 4) if run64 == "r4" else (3 * K + 3),
+            "gpu_launches": (4 * K + 4) if run64 in ("r4", "r4t") else (3 * K + 3),
             "finite": finite, "roofline": roofline, "clocks": clocks,
             "e2e": {"value": ws * K / (e2e_ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d / K,
                     "d2h_bytes_per_step": d2h / K,

@@ -130,7 +130,7 @@ template <> __device__ __forceinline__ void make_tw<float2>(float2* tw) { quad64
 }  // namespace r4
 
 template <class C>
-constexpr size_t r4_smem_bytes() { return sizeof(C) * (64 * 64 + 64); }
+constexpr size_t r4_smem_bytes() { return sizeof(C) * (64 * 64 + 64) + sizeof(double2) * 128; }
 
 // One half-step, one plane per CTA (blockIdx = f0 * 64 + f1).
 //   KIN: src LA -> dst LB, factor scale / norm;
@@ -149,6 +149,7 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
     extern __shared__ __align__(16) unsigned char smraw[];
     C* s = reinterpret_cast<C*>(smraw);
     C* tw = s + 64 * 64;
+    double2* pvs = reinterpret_cast<double2*>(tw + 64);         // this plane's factor vectors
     const int t = threadIdx.x, pl = blockIdx.x, f0 = pl >> 6, f1 = pl & 63;
     const int ac = t & 15, ar = t >> 4;
     C v[16];
@@ -161,10 +162,11 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
                 v[4 * i + j] = g[(long long)i * (16LL * 64 * 64 * 64) + (long long)j * (16LL * 64 * 64)];
     }
     if (t < 64) tw[t] = gtw[t];
+    if (t < 128) pvs[t] = __ldg(PV + (long long)pl * 128 + t);
     double2 cc = scale;
     if (KIN && d_norm) cc = zmul(cc, zinv(make_double2(d_norm[0], d_norm[1])));
     const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
-    __syncthreads();                                           // twiddles ready
+    __syncthreads();                                           // twiddles and factor vectors ready
     // ---- forward
     pass<C, true>(v);
     twiddle<C, true>(v, tw, ac, ar);
@@ -181,13 +183,12 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
     // ---- factor at kc = c2 + 4 c1 + 16 j, kr = r2 + 4 r1 + 16 i
     {
         const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
-        const double2* pv = PV + (long long)pl * 128;
         double2 b[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = __ldg(pv + 64 + c2 + 4 * c1 + 16 * j);
+        for (int j = 0; j < 4; ++j) b[j] = pvs[64 + c2 + 4 * c1 + 16 * j];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const double2 a = zmul(__ldg(pv + r2 + 4 * r1 + 16 * i), cc);
+            const double2 a = zmul(pvs[r2 + 4 * r1 + 16 * i], cc);
 #pragma unroll
             for (int j = 0; j < 4; ++j) factor_mul(v[4 * i + j], a, b[j]);
         }

@@ -542,6 +542,7 @@ __global__ void __launch_bounds__(lanes64::NT, 2) k_pot64(const C* __restrict__ 
 //   all of its planes; one partial row per CTA.
 // ---------------------------------------------------------------------------
 #define NSUM 22   // sum W, xW, x^2 W, p_x W, p_x^2 W, yW, y^2 W, p_y W, p_y^2 W, K W, V W (complex)
+#define FOLD_BLOCKS 64   // first-stage rows of the Run() reduction over columns
 
 // Per-plane factor vectors, built once at plan creation: for plane (f0, f1)
 // the row-frequency vector PV[plane][0][k] and the column-frequency vector
@@ -780,6 +781,50 @@ __global__ void __launch_bounds__(32 * NSUM) k_finalize_sums(const double* __res
 #include "quad64.cuh"
 #include "r4.cuh"
 
+// First stage of the Run() reduction for one partial row per column (y, x):
+// CTA b folds the columns b*per .. b*per + per - 1, weighted by x, y and V of
+// each column, into one NSUM row (the layout k_finalize_sums reads).  Two
+// small launches instead of one single-CTA pass over every column.
+__global__ void __launch_bounds__(256) k_fold_columns(const double* __restrict__ part, int ncols, int nx, int per,
+                                                      ObsTabs ob, double* __restrict__ rows) {
+    __shared__ double red[NSUM][8];
+    double a[NSUM];
+#pragma unroll
+    for (int i = 0; i < NSUM; ++i) a[i] = 0.0;
+    const int c0 = blockIdx.x * per, c1 = min(ncols, c0 + per);
+    for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+        const int ix = c % nx, iy = c / nx;
+        const double x = __ldg(ob.cx + ix), y = __ldg(ob.cy + iy), V = __ldg(ob.ex + c);
+        const double* p = part + (long long)c * NPART;
+        const double wr = p[0], wi = p[1];
+        a[0] += wr;               a[1] += wi;                 // W
+        a[2] = fma(x, wr, a[2]);  a[3] = fma(x, wi, a[3]);    // x W
+        a[4] = fma(x * x, wr, a[4]); a[5] = fma(x * x, wi, a[5]);
+        a[6] += p[2];             a[7] += p[3];               // p_x W
+        a[8] += p[4];             a[9] += p[5];               // p_x^2 W
+        a[10] = fma(y, wr, a[10]); a[11] = fma(y, wi, a[11]); // y W
+        a[12] = fma(y * y, wr, a[12]); a[13] = fma(y * y, wi, a[13]);
+        a[14] += p[6];            a[15] += p[7];              // p_y W
+        a[16] += p[8];            a[17] += p[9];              // p_y^2 W
+        a[18] += p[10];           a[19] += p[11];             // K W
+        a[20] = fma(V, wr, a[20]); a[21] = fma(V, wi, a[21]); // V W
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < NSUM; ++i) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a[i] += __shfl_down_sync(0xffffffffu, a[i], o);
+        if (l == 0) red[i][w] = a[i];
+    }
+    __syncthreads();
+    if (threadIdx.x < NSUM) {
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) t += red[threadIdx.x][k];
+        rows[(long long)blockIdx.x * NSUM + threadIdx.x] = t;
+    }
+}
+
 // Standalone reduction of a state in the (x, p) representation: same CTA
 // shape and partial layout as k_potential's epilogue.
 template <class C, int NT>
@@ -960,6 +1005,7 @@ struct wig4d_plan {
     bool r4t;                      // complex128 64^4 Run(): k_r4 with TMA plane loads (k_r4t)
     bool r4_cluster;               // k_r4 launched as clusters with full-sector stores
     void* tw64;                    // k_r4 twiddle table (64 complex of the plan's dtype)
+    double* fold;                  // k_fold_columns output: FOLD_BLOCKS rows of NSUM
     CUtensorMap map_t_load;        // LA view of the ping-pong buffer (kinetic source)
     CUtensorMap map_w_load;        // LB view of the caller's state (potential source)
     const void* map_w_ptr;                 // state the W maps describe
@@ -1128,6 +1174,7 @@ static void free_plan(wig4d_plan* p) {
     cudaFree(p->pingpong);
     cudaFree(p->pv);
     cudaFree(p->tw64);
+    cudaFree(p->fold);
     delete p;
 }
 
@@ -1381,6 +1428,7 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             p->quad64 = false;
             p->r4_cluster = !(kern && strcmp(kern, "r4") == 0);
             if (cudaMalloc(&p->tw64, 64 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+            if (cudaMalloc(&p->fold, FOLD_BLOCKS * NSUM * sizeof(double)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
             if (desc->dtype == WIG_C128) k_make_r4_twiddles<double2><<<1, 64>>>((double2*)p->tw64);
             else k_make_r4_twiddles<float2><<<1, 64>>>((float2*)p->tw64);
             const int rsm = (int)(desc->dtype == WIG_C128 ? r4_smem_bytes<double2>() : r4_smem_bytes<float2>());
@@ -1556,6 +1604,19 @@ extern "C" int wig4d_observables_noalloc(const void* W, const int shape[4], int 
 
 // One Run() iteration in three parts: kinetic (dividing by the current norm),
 // potential with the partial sums of the new state, finalize into the history.
+// Run() reduction of k_r4's per-column partial rows: fold into FOLD_BLOCKS
+// rows, then k_finalize_sums (norm, observables row, current norm, counter).
+static int fold_and_finalize(wig4d_plan* p, double* hist, int rows, cudaStream_t st) {
+    const int ncols = p->shape[1] * p->shape[3];
+    const int per = (ncols + FOLD_BLOCKS - 1) / FOLD_BLOCKS;
+    k_fold_columns<<<FOLD_BLOCKS, 256, 0, st>>>(p->partials, ncols, p->shape[3], per, p->ob, p->fold);
+    WIG_LAUNCHED("k_fold_columns");
+    k_finalize_sums<<<1, 32 * NSUM, 0, st>>>(p->fold, FOLD_BLOCKS, p->dv_norm, p->dv_obs, hist, p->counter, rows,
+                                             p->cur_norm, p->flag);
+    WIG_LAUNCHED("k_finalize_sums");
+    return WIG_OK;
+}
+
 // k_r4 launch: with clusters of IL CTAs (full-sector stores) or plain.
 template <class C, bool KIN>
 static cudaError_t launch_r4(bool cluster, unsigned grid, size_t sm, cudaStream_t st, const C* src, C* dst,
@@ -1601,7 +1662,7 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
                                                           p->partials);
                 WIG_LAUNCHED("k_r4t<pot>");
             } else {
-                return finalize(p, hist, p->counter, rows, st);
+                return fold_and_finalize(p, hist, rows, st);
             }
             return WIG_OK;
         }
@@ -1622,7 +1683,7 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
                                           make_double2(p->pot_scale, 0.0), nullptr, p->ob, p->partials)));
             WIG_LAUNCHED("k_r4<pot>");
         } else {
-            return finalize(p, hist, p->counter, rows, st);
+            return fold_and_finalize(p, hist, rows, st);
         }
         return WIG_OK;
     }
