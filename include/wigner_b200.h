@@ -232,7 +232,8 @@ int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
    kinetic half-step, info[1] fused potential half-step, info[2] the 64^4
    Run() kernels (1 or 0 each); info[3] which 64^4 Run() kernels: 0 none,
    1 k_half64 (plane pairs), 2 k_quad64 (complex64 quads), 3 k_r4 (16 points
-   per thread, the default), 4 k_r4t (complex128 k_r4 with TMA plane loads). */
+   per thread, the default), 4 k_r4t (complex128 k_r4 with TMA plane loads),
+   5 k_r4p (persistent k_r4 with the next plane prefetched). */
 int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
 
 /* Bytes of device memory the plan holds (tables, partial sums). */

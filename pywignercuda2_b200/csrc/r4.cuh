@@ -493,3 +493,171 @@ k_r4t(const __grid_constant__ CUtensorMap src_map, double2* __restrict__ dst,
 // The 64-entry twiddle table of k_r4 / k_r4t, built once per plan.
 template <class C>
 __global__ void k_make_r4_twiddles(C* tw) { r4::make_tw<C>(tw); }
+
+// ---------------------------------------------------------------------------
+// k_r4p: k_r4 as a persistent kernel that overlaps each plane's transforms
+// with the load of its next plane.
+//
+// A CTA loops over the planes blockIdx.x + k * gridDim.x with two plane
+// buffers B0, B1 in shared memory.  At iteration k the plane is in B[k&1]
+// (copied there by cp.async during iteration k-1, straight from global
+// memory without passing through registers); the thread reads its 16 points,
+// issues the copies of the next plane (and its factor vectors) into
+// B[(k+1)&1], and then uses B[k&1] for the four exchanges, the reduction and
+// the cluster staging.  B[(k+1)&1] is free at that moment: its last readers,
+// the partner CTAs of the previous iteration's cluster stores, finished
+// before that iteration's final cluster barrier.  Clusters keep their IL
+// CTAs on the same quad of planes because gridDim.x and the plane count are
+// multiples of IL.
+// ---------------------------------------------------------------------------
+template <class C>
+constexpr size_t r4p_smem_bytes() { return sizeof(C) * (2 * 64 * 64 + 64) + sizeof(double2) * 2 * 128; }
+
+template <class C, bool KIN>
+__global__ void __launch_bounds__(r4::NT, (sizeof(C) == 16 ? 1 : 3))
+k_r4p(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__ PV, const C* __restrict__ gtw,
+      double2 scale, const double* __restrict__ d_norm, ObsTabs ob, double* __restrict__ partials) {
+    using namespace r4;
+    namespace cg = cooperative_groups;
+    constexpr int IL = Il<C>::v, NQ = 64 / IL, NP = 64 * 64;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* buf0 = reinterpret_cast<C*>(smraw);
+    C* tw = buf0 + 2 * 64 * 64;
+    double2* pvb = reinterpret_cast<double2*>(tw + 64);        // [2][128]
+    const int t = threadIdx.x, ac = t & 15, ar = t >> 4;
+    cg::cluster_group cl = cg::this_cluster();
+    const int q = (int)cl.block_rank();
+    // this thread's 16 points of plane (f0, f1): src offsets relative to the plane base
+    auto prefetch = [&](int pl, int b) {
+        const int f0 = pl >> 6, f1 = pl & 63;
+        const C* g = src + ((((long long)ar * NQ + ac / IL) * 64 + f0) * 64 + f1) * IL + (ac % IL);
+        C* d = buf0 + b * 64 * 64;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                cp_async_elem(d + (ar + 16 * i) * 64 + ac + 16 * j,
+                              g + (long long)i * (16LL * 64 * 64 * 64) + (long long)j * (16LL * 64 * 64));
+        if (t < 128)
+            cp_async_elem(pvb + b * 128 + t, PV + (long long)pl * 128 + t);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (t < 64) tw[t] = gtw[t];
+    double2 cc = scale;
+    if (KIN && d_norm) cc = zmul(cc, zinv(make_double2(d_norm[0], d_norm[1])));
+    const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
+    if (blockIdx.x < NP) prefetch(blockIdx.x, 0);
+    int k = 0;
+    for (int pl = blockIdx.x; pl < NP; pl += gridDim.x, ++k) {
+        const int cur = k & 1, f0 = pl >> 6, f1 = pl & 63;
+        C* s = buf0 + cur * 64 * 64;
+        const double2* pvs = pvb + cur * 128;
+        cp_async_wait_all();
+        __syncthreads();                                     // plane, factor vectors (and twiddles) in place
+        C v[16];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[4 * i + j] = s[(ar + 16 * i) * 64 + ac + 16 * j];
+        if (pl + (int)gridDim.x < NP) prefetch(pl + gridDim.x, cur ^ 1);
+        // ---- forward
+        pass<C, true>(v);
+        twiddle<C, true>(v, tw, ac, ar);
+        __syncthreads();                                     // the plane has been read
+        put(s, L1, v);
+        __syncthreads();
+        get(s, L2, v);
+        pass<C, true>(v);
+        twiddle<C, true>(v, tw, 4 * (t & 3), 4 * ((t >> 4) & 3));
+        __syncthreads();
+        put(s, L2, v);
+        __syncthreads();
+        get(s, L3, v);
+        pass<C, true>(v);
+        {
+            const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
+            double2 b[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = pvs[64 + c2 + 4 * c1 + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const double2 a = zmul(pvs[r2 + 4 * r1 + 16 * i], cc);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) factor_mul(v[4 * i + j], a, b[j]);
+            }
+        }
+        // ---- inverse
+        pass<C, false>(v);
+        twiddle<C, false>(v, tw, ((t >> 2) & 3) + 4 * (t & 3), (t >> 6) + 4 * ((t >> 4) & 3));
+        __syncthreads();
+        put(s, L3, v);
+        __syncthreads();
+        get(s, L2, v);
+        pass<C, false>(v);
+        twiddle<C, false>(v, tw, 4 * ((t >> 2) & 3), 4 * (t >> 6));
+        __syncthreads();
+        put(s, L2, v);
+        __syncthreads();
+        get(s, L1, v);
+        pass<C, false>(v);
+        if (!KIN) {
+            typedef typename real_of<C>::type R;
+            R a[NPART];
+#pragma unroll
+            for (int m = 0; m < NPART; ++m) a[m] = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const R qy = (R)__ldg(ob.cpy + ar + 16 * i);
+                R w0x = 0, w0y = 0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const C w = v[4 * i + j];
+                    const R qx = (R)__ldg(ob.cpx + ac + 16 * j), kk = (R)__ldg(ob.ep + (ar + 16 * i) * 64 + ac + 16 * j);
+                    w0x += w.x; w0y += w.y;
+                    a[2] += qx * w.x; a[3] += qx * w.y;
+                    a[4] += qx * qx * w.x; a[5] += qx * qx * w.y;
+                    a[10] += kk * w.x; a[11] += kk * w.y;
+                }
+                a[0] += w0x; a[1] += w0y;
+                a[6] += qy * w0x; a[7] += qy * w0y;
+                a[8] += qy * qy * w0x; a[9] += qy * qy * w0y;
+            }
+            double* red = reinterpret_cast<double*>(s);
+            __syncthreads();                                 // last exchange read
+#pragma unroll
+            for (int m = 0; m < NPART; ++m) red[m * NT + t] = (double)a[m];
+            __syncthreads();
+            const int w = t >> 5, l = t & 31;
+            for (int m = w; m < NPART; m += NT / 32) {
+                double sum = 0.0;
+#pragma unroll
+                for (int u = 0; u < NT / 32; ++u) sum += red[m * NT + u * 32 + l];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+                if (l == 0) partials[(long long)pl * NPART + m] = sum;
+            }
+        }
+        // ---- cluster stores (as k_r4): stage, gather the IL planes, whole sectors
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) s[(ar + 16 * i) * 64 + ac + 16 * j] = v[4 * i + j];
+        cl.sync();
+        const C* part[IL];
+#pragma unroll
+        for (int g = 0; g < IL; ++g) part[g] = cl.map_shared_rank(s, g);
+        C* gb = dst + ((long long)f0 * NQ + f1 / IL) * 64 * 64 * IL;
+        constexpr int PER = 4096 / IL / NT;
+#pragma unroll
+        for (int m = 0; m < PER; ++m) {
+            const int pt = q * (4096 / IL) + m * NT + t;
+            C val[IL];
+#pragma unroll
+            for (int g = 0; g < IL; ++g) val[g] = part[g][pt];
+            st_sector(gb + (long long)pt * IL, val);
+        }
+        cl.sync();                                           // partners done reading this buffer
+    }
+    cp_async_wait_all();
+}

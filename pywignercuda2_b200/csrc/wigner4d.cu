@@ -1004,6 +1004,8 @@ struct wig4d_plan {
     bool r4;                       // 64^4 Run(): k_r4 (16 points per thread) on its LA / LB layouts
     bool r4t;                      // complex128 64^4 Run(): k_r4 with TMA plane loads (k_r4t)
     bool r4_cluster;               // k_r4 launched as clusters with full-sector stores
+    bool r4p;                      // persistent k_r4p (next plane prefetched by cp.async)
+    int r4p_grid;                  // its CTAs: SMs x resident CTAs, a multiple of the cluster size
     void* tw64;                    // k_r4 twiddle table (64 complex of the plan's dtype)
     double* fold;                  // k_fold_columns output: FOLD_BLOCKS rows of NSUM
     CUtensorMap map_t_load;        // LA view of the ping-pong buffer (kinetic source)
@@ -1429,6 +1431,23 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             p->r4_cluster = !(kern && strcmp(kern, "r4") == 0);
             if (cudaMalloc(&p->tw64, 64 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
             if (cudaMalloc(&p->fold, FOLD_BLOCKS * NSUM * sizeof(double)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+            p->r4p = kern && strcmp(kern, "r4p") == 0;
+            if (p->r4p) {
+                const int psm = (int)(desc->dtype == WIG_C128 ? r4p_smem_bytes<double2>() : r4p_smem_bytes<float2>());
+                const int il = desc->dtype == WIG_C128 ? 2 : 4;
+                int occ = 0;
+                if (desc->dtype == WIG_C128) {
+                    cudaFuncSetAttribute(k_r4p<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm);
+                    cudaFuncSetAttribute(k_r4p<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm);
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_r4p<double2, false>, r4::NT, psm);
+                } else {
+                    cudaFuncSetAttribute(k_r4p<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm);
+                    cudaFuncSetAttribute(k_r4p<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm);
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_r4p<float2, false>, r4::NT, psm);
+                }
+                if (occ < 1) occ = 1;
+                p->r4p_grid = (wig_num_sms() * occ / il) * il;
+            }
             if (desc->dtype == WIG_C128) k_make_r4_twiddles<double2><<<1, 64>>>((double2*)p->tw64);
             else k_make_r4_twiddles<float2><<<1, 64>>>((float2*)p->tw64);
             const int rsm = (int)(desc->dtype == WIG_C128 ? r4_smem_bytes<double2>() : r4_smem_bytes<float2>());
@@ -1468,7 +1487,7 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     if (!p || !info) return WIG_ERR_INVALID_ARG;
     info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64;
-    info[3] = !p->fast64 ? 0 : (p->r4t ? 4 : (p->r4 ? 3 : (p->quad64 ? 2 : 1)));
+    info[3] = !p->fast64 ? 0 : (p->r4p ? 5 : (p->r4t ? 4 : (p->r4 ? 3 : (p->quad64 ? 2 : 1))));
     return WIG_OK;
 }
 
@@ -1617,6 +1636,25 @@ static int fold_and_finalize(wig4d_plan* p, double* hist, int rows, cudaStream_t
     return WIG_OK;
 }
 
+// k_r4p launch: persistent, clusters of IL CTAs.
+template <class C, bool KIN>
+static cudaError_t launch_r4p(unsigned grid, cudaStream_t st, const C* src, C* dst, const double2* pv, const C* tw,
+                              double2 scale, const double* d_norm, ObsTabs ob, double* partials) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(r4::NT);
+    cfg.dynamicSmemBytes = r4p_smem_bytes<C>();
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = r4::Il<C>::v;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_r4p<C, KIN>, src, dst, pv, tw, scale, d_norm, ob, partials);
+}
+
 // k_r4 launch: with clusters of IL CTAs (full-sector stores) or plain.
 template <class C, bool KIN>
 static cudaError_t launch_r4(bool cluster, unsigned grid, size_t sm, cudaStream_t st, const C* src, C* dst,
@@ -1673,6 +1711,17 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
         const double2* pv = reinterpret_cast<const double2*>(p->pv);
         constexpr size_t sm = r4_smem_bytes<C>();
         const unsigned nplanes = 64 * 64;
+        if (p->r4p && part < 2) {
+            if (part == 0)
+                WIG_CUDA((launch_r4p<C, true>(p->r4p_grid, st, P, W, pv, (const C*)p->tw64,
+                                              make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr)));
+            else
+                WIG_CUDA((launch_r4p<C, false>(p->r4p_grid, st, W, P, pv + (size_t)p->shape[0] * p->shape[2] * 128,
+                                               (const C*)p->tw64, make_double2(p->pot_scale, 0.0), nullptr, p->ob,
+                                               p->partials)));
+            WIG_LAUNCHED("k_r4p");
+            return WIG_OK;
+        }
         if (part == 0) {
             WIG_CUDA((launch_r4<C, true>(p->r4_cluster, nplanes, sm, st, P, W, pv, (const C*)p->tw64,
                                          make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr)));

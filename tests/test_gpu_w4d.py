@@ -319,3 +319,25 @@ def test_r4_variants_match_default(variant, monkeypatch):
     for name in OBS:
         assert rel_err(getattr(f1, name), getattr(f2, name)) < 1e-13, name
     assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < 1e-12
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_r4p_matches_r4(dtype, monkeypatch):
+    """The persistent k_r4p (next plane prefetched) runs k_r4's arithmetic
+    plane by plane: the same history and state."""
+    from configs import cat_xp
+    p, c = config2(8, 64)
+    f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    monkeypatch.setenv("WIG_FAST64_KERNEL", "r4p")
+    f2 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    monkeypatch.delenv("WIG_FAST64_KERNEL")
+    assert (f1.plan_info()["run64_kernel"], f2.plan_info()["run64_kernel"]) == ("r4", "r4p")
+    W0 = cat_xp(f1._coords, c).astype(dtype)
+    for f in (f1, f2):
+        f.W_init_gpu.set(W0)
+        f.timeSteps = 9
+        f.fileName = None
+        f.Run()
+    for name in OBS:
+        assert rel_err(getattr(f1, name), getattr(f2, name)) < 1e-13, name
+    assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < 1e-13
