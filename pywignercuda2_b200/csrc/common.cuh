@@ -76,3 +76,14 @@ int wig_num_sms();
 
 // Line lengths with a radix transform (Stockham passes of radix 8/4/3/2).
 static inline bool wig_radix_size(int n) { return n == 16 || n == 32 || n == 48 || n == 64 || n == 128; }
+
+// Asynchronous global -> shared copies of one complex element (cp.async).
+__device__ __forceinline__ void cp_async_elem(double2* dst, const double2* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(float2* dst, const float2* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }

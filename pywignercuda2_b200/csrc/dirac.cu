@@ -17,6 +17,7 @@
 // two slots (the reference's Run() binds W21 to W22) gets the reference's
 // result; the C ABI accepts that only for the elementwise entry points.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -516,6 +517,55 @@ __global__ void __launch_bounds__(NT) k_dplane(Slots<C> S, int n0, int n1, int n
     }
 }
 
+// KIND 1 over G neighbouring columns i3 per CTA.  A (axis 0, axis 2) plane at
+// fixed (i1, i3) is a gather at stride N_3; G = 32 bytes / element makes every
+// access one whole 32-byte sector, copied by cp.async straight into shared
+// memory.  The centring signs are folded into the store:
+//   S DFT2(S v)[k] = (-1)^(ka + kb) DFT2(v)[k + N/2],
+// so the transform reads its plane unsigned and the store reads the result
+// at frequencies shifted by N/2.
+template <int NA, int LD>
+struct DPlaneG {
+    static constexpr int PSP = ((NA * LD + 13) / 16) * 16 + 2;   // plane stride, = 2 (mod 16)
+};
+template <class C, int NA, int NB, int NT, bool FWD, int G>
+__global__ void __launch_bounds__(NT) k_dplane_g(Slots<C> S, int n0, int n1, int n2, int n3, double2 scale,
+                                                 const double* __restrict__ d_norm) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    constexpr int LD = NB + 1, PSP = DPlaneG<NA, LD>::PSP;
+    C* s = reinterpret_cast<C*>(smraw);
+    C* twb = s + G * PSP;
+    C* twa = twb + NB;
+    const int n3g = n3 / G;
+    const int i3 = (blockIdx.x % n3g) * G, i1 = blockIdx.x / n3g;
+    const long long rs = (long long)n1 * n2 * n3, cs = n3;
+    C* g0 = S.p[blockIdx.y] + (long long)i1 * n2 * n3 + i3;
+    for (int e = threadIdx.x; e < G * NA * NB; e += NT) {
+        const int g = e % G, b = (e / G) % NB, a = e / (G * NB);
+        cp_async_elem(s + g * PSP + a * LD + b, g0 + a * rs + b * cs + g);
+    }
+    make_twiddles(twb, NB);
+    if (NA != NB) make_twiddles(twa, NA);
+    const C* ta = (NA != NB) ? twa : twb;
+    double2 sc = scale;
+    if (d_norm) sc = zmul(sc, zinv(make_double2(d_norm[0], d_norm[1])));
+    const C cc = to_c<C>(sc);
+    cp_async_wait_all();
+    __syncthreads();
+    const LineMap rows{1, LD, 0, 1}, cols{1, 1, 0, LD};
+    for (int g = 0; g < G; ++g) {
+        fft_lines<C, NB, NA, NT, FWD, true>(s + g * PSP, rows, twb);
+        fft_lines<C, NA, NB, NT, FWD, true>(s + g * PSP, cols, ta);
+    }
+    for (int e = threadIdx.x; e < G * NA * NB; e += NT) {
+        const int g = e % G, b = (e / G) % NB, a = e / (G * NB);
+        const int sa = (a + NA / 2) % NA, sb = (b + NB / 2) % NB;
+        C v = cmul(s[g * PSP + sa * LD + sb], cc);
+        if ((a + b) & 1) v = cneg(v);
+        g0[a * rs + b * cs + g] = v;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Plan
 // ---------------------------------------------------------------------------
@@ -813,9 +863,21 @@ static int launch_dplane(wigd_plan* p, const Slots<C>& S, int nslots, double2 sc
     const int NB = KIND == 0 ? p->d.shape[3] : p->d.shape[2];
     const unsigned planes = KIND == 0 ? (unsigned)(p->d.shape[0] * p->d.shape[2]) : (unsigned)(p->d.shape[1] * p->d.shape[3]);
     dim3 grid(planes, nslots);
+    constexpr int G = 32 / (int)sizeof(C);
 #define DCASE(a, b)                                                                              \
     if (NA == a && NB == b) {                                                                    \
         constexpr int NT = (a * b / 8 >= 512) ? 512 : 256;                                       \
+        if (KIND == 1 && p->d.shape[3] % G == 0 && !getenv("WIG_NO_DPLANE_G")) {                 \
+            auto kg = k_dplane_g<C, a, b, NT, FWD, G>;                                           \
+            const size_t smg = sizeof(C) * ((size_t)G * DPlaneG<a, b + 1>::PSP + a + b);         \
+            if (smg <= 227 * 1024) {                                                             \
+                WIG_CUDA(cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg)); \
+                kg<<<dim3(planes / G, nslots), NT, smg, st>>>(S, p->d.shape[0], p->d.shape[1],   \
+                                                              p->d.shape[2], p->d.shape[3], sc, d_norm); \
+                WIG_LAUNCHED("k_dplane_g");                                                      \
+                return WIG_OK;                                                                   \
+            }                                                                                    \
+        }                                                                                        \
         auto kern = k_dplane<C, a, b, NT, KIND, FWD>;                                            \
         const size_t sm = sizeof(C) * ((size_t)a * (b + 1) + a + b);                             \
         if (sm > 227 * 1024) return WIG_ERR_UNSUPPORTED;                                        \

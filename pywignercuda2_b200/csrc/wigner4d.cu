@@ -299,15 +299,6 @@ struct PotCfg {
     }
 };
 
-__device__ __forceinline__ void cp_async_elem(double2* dst, const double2* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_elem(float2* dst, const float2* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 template <class C, int NPY, int NPX, int G>
 __global__ void __launch_bounds__(256, 1) k_potential_g(C* __restrict__ W, int ny, int nx, FactorSet<C> F,
