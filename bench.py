@@ -35,10 +35,8 @@ WORKLOAD = "GPU_Wigner4D plain complex128 Run() iteration, 64x64x64x64, cat stat
 
 
 def _dist():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from pywignercuda2_b200.replicas import rank_info
+    return rank_info()
 
 
 def _clock_sampler(local):
@@ -135,28 +133,33 @@ def bench_batched(steps):
     """The batched workload: 48 instances (16 each at 32^4, 48^4, 64^4, own
     coefficients, centres, D and dt) advanced together in complex64 through
     WignerBatch, against the same 48 run one at a time in the plain complex128
-    form.  Aggregate grid-point steps per second, CUDA events."""
+    form.  Aggregate grid-point steps per second, CUDA events.  With N ranks
+    the instances are split among them (no collective on the data path): the
+    job's time is the slowest rank's, its points the sum over ranks."""
     import torch
     from configs import config4, gaussian_xp
     from frames import make_frame
-    from pywignercuda2_b200 import GPU_Wigner4D, WignerBatch
-    cfg = config4(0)
+    from pywignercuda2_b200 import GPU_Wigner4D, WignerBatch, replicas
+    ws, rank, _ = replicas.rank_info()
+    cfg = replicas.shard(config4(0), rank, ws)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     frames = []
     for params, c in cfg:
         f = make_frame(GPU_Wigner4D, dict(params, timeSteps=steps - 1), complex_dtype=np.complex64)
         f.W_init_gpu.set(gaussian_xp(f._coords, c).astype(np.complex64))
         frames.append(f)
-    pts = sum(int(np.prod(f.shape)) for f in frames)
+    pts_rank = sum(int(np.prod(f.shape)) for f in frames)
+    pts = int(replicas.sum_over_ranks(pts_rank))
     batch = WignerBatch(frames)
     hists = [torch.empty((steps, 11), dtype=torch.float64, device="cuda") for _ in frames]
     batch.run_device(3, hists)
     torch.cuda.synchronize()
+    replicas.barrier()
     e0.record()
     batch.run_device(steps, hists)
     e1.record()
     torch.cuda.synchronize()
-    ms_batch = e0.elapsed_time(e1)
+    ms_batch = replicas.max_over_ranks(e0.elapsed_time(e1))
     finite = all(bool(torch.isfinite(h).all()) for h in hists)
     del batch, frames, hists
     ms_plain = 0.0
@@ -172,9 +175,11 @@ def bench_batched(steps):
         torch.cuda.synchronize()
         ms_plain += e0.elapsed_time(e1)
         del f, h
+    ms_plain = replicas.max_over_ranks(ms_plain)
     return {"workload": "48 instances: 16 x 32^4, 16 x 48^4, 16 x 64^4, seeded q, kappa, centre, "
                         "D in U[0.001, 0.02], dt in {0.005, 0.01}", "steps": steps,
-            "grid_points": pts, "dtype": "c64",
+            "grid_points": pts, "dtype": "c64", "ranks": ws,
+            "scaling": "strong", "parallelism": "instances split over ranks" if ws > 1 else "single",
             "gp_steps_per_s": pts * steps / (ms_batch / 1e3), "ms": ms_batch, "finite": finite,
             "one_at_a_time_plain_c128": {"gp_steps_per_s": pts * steps / (ms_plain / 1e3), "ms": ms_plain},
             "speedup_vs_one_at_a_time_plain": ms_plain / ms_batch}
@@ -279,7 +284,7 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    from pywignercuda2_b200 import _lib
+    from pywignercuda2_b200 import _lib, replicas
 
     K, Wm = args.steps, args.warmup
     f, W0 = _frame(np.complex128)
@@ -288,8 +293,7 @@ def main():
     hist = torch.empty((K + Wm + 2, _lib.WIG4D_NOBS), dtype=torch.float64, device="cuda")
 
     def barrier():
-        if ws > 1:
-            dist.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
 
     # ---- device-resident throughput (value) ---------------------------------
@@ -304,10 +308,7 @@ def main():
     barrier()
     ms = e0.elapsed_time(e1)
     clocks = _clock_summary(clk)
-    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = replicas.max_over_ranks(ms)
     value = ws * K / (ms / 1e3)
     h128 = hist[:K].cpu().numpy()
     finite = bool(np.all(np.isfinite(h128)))
@@ -395,11 +396,7 @@ def main():
     host_out.copy_(f.W_init_gpu.tensor, non_blocking=True)
     e1.record(st)
     barrier()
-    e2e_ms = e0.elapsed_time(e1)
-    t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t.item())
+    e2e_ms = replicas.max_over_ranks(e0.elapsed_time(e1))
     h2d = state_bytes
     d2h = state_bytes + K * _lib.WIG4D_NOBS * 8
 
