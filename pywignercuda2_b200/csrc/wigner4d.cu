@@ -770,6 +770,7 @@ __global__ void __launch_bounds__(32 * NSUM) k_finalize_sums(const double* __res
 }
 
 #include "quad64.cuh"
+#include "dense_half.cuh"
 #include "r4.cuh"
 
 // First stage of the Run() reduction for one partial row per column (y, x):
@@ -996,6 +997,8 @@ struct wig4d_plan {
     bool r4t;                      // complex128 64^4 Run(): k_r4 with TMA plane loads (k_r4t)
     bool r4_cluster;               // k_r4 launched as clusters with full-sector stores
     bool r4p;                      // persistent k_r4p (next plane prefetched by cp.async)
+    int dense_n;                   // > 0: general-delta half-steps fused (k_dense_half, N^4 grids)
+    const void* dmat[4];           // FAFT matrices per axis (|delta|), when dense_n > 0
     int r4p_grid;                  // its CTAs: SMs x resident CTAs, a multiple of the cluster size
     void* tw64;                    // k_r4 twiddle table (64 complex of the plan's dtype)
     double* fold;                  // k_fold_columns output: FOLD_BLOCKS rows of NSUM
@@ -1123,15 +1126,42 @@ static int halfstep_unfused(wig4d_plan* p, C* W, int which, const double* d_norm
     return WIG_OK;
 }
 
+// Fused general-delta half-step (k_dense_half), N^4 grids with N = 16, 32, 64.
+template <class C, bool KIN>
+static int launch_dense(wig4d_plan* p, C* W, const double* d_norm, double* partials, cudaStream_t st) {
+    const int ar = KIN ? 1 : 0, ac = KIN ? 3 : 2;          // row / column axes of the plane
+    const C* Mr = reinterpret_cast<const C*>(p->dmat[ar]);
+    const C* Mc = reinterpret_cast<const C*>(p->dmat[ac]);
+    const int n = p->dense_n;
+    const unsigned grid = (unsigned)(n * n);
+    const double2 sc = make_double2(KIN ? p->kin_scale : p->pot_scale, 0.0);
+    FactorSet<C>& F = KIN ? kin_set<C>(p) : pot_set<C>(p);
+#define DENSE_CASE(N)                                                                                  \
+    if (n == N) {                                                                                      \
+        auto kern = k_dense_half<C, N, KIN>;                                                           \
+        const size_t sm = dense_half_smem_bytes<C, N>(Mr != Mc);                                      \
+        WIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));    \
+        kern<<<grid, dense_half::NT, sm, st>>>(W, n, Mr, Mc, p->delta[ar] < 0, p->delta[ac] < 0, F, sc, d_norm, \
+                                               p->ob, partials, n);                                    \
+        WIG_LAUNCHED("k_dense_half");                                                                  \
+        return WIG_OK;                                                                                 \
+    }
+    DENSE_CASE(16) DENSE_CASE(32) DENSE_CASE(64)
+#undef DENSE_CASE
+    return WIG_ERR_UNSUPPORTED;
+}
+
 template <class C>
 static int kinetic_impl(wig4d_plan* p, C* W, const double* d_norm, cudaStream_t st) {
     if (p->fused_kin) return launch_kinetic<C>(p, W, d_norm, st);
+    if (p->dense_n) return launch_dense<C, true>(p, W, d_norm, nullptr, st);
     return halfstep_unfused<C>(p, W, 0, d_norm, st);
 }
 
 template <class C>
 static int potential_impl(wig4d_plan* p, C* W, double* partials, cudaStream_t st) {
     if (p->fused_pot) return launch_potential<C>(p, W, partials, st);
+    if (p->dense_n) return launch_dense<C, false>(p, W, nullptr, partials, st);
     int s = halfstep_unfused<C>(p, W, 1, nullptr, st);
     if (s || !partials) return s;
     k_reduce_xp<C, 256><<<p->shape[1] * p->shape[3], 256, 0, st>>>(
@@ -1335,6 +1365,22 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
     for (int a = 0; a < 4; ++a) {
         const bool fast = pow2_16_128(p->shape[a]) && fabs(fabs(p->delta[a]) * p->shape[a] - 1.0) < 1e-12;
         if (!fast && !wig_dense_matrix(p->shape[a], fabs(p->delta[a]), p->dtype, 0)) { free_plan(p); return WIG_ERR_ALLOC; }
+    }
+    // general delta on an N^4 grid (N = 16, 32, 64): both half-steps fused
+    // (k_dense_half) when neither is on the radix path
+    {
+        const int n = p->shape[0];
+        const bool square = p->shape[1] == n && p->shape[2] == n && p->shape[3] == n;
+        if (square && (n == 16 || n == 32 || n == 64) && !p->fused_kin && !p->fused_pot &&
+            getenv("WIG_NO_DENSE_FUSED") == nullptr) {
+            bool ok = true;
+            for (int a = 0; a < 4; ++a) {
+                p->dmat[a] = wig_dense_matrix(n, fabs(p->delta[a]), p->dtype, 0);
+                ok = ok && p->dmat[a];
+            }
+            if (!ok) { free_plan(p); return WIG_ERR_ALLOC; }
+            p->dense_n = n;
+        }
     }
     // the 64^4 kernels take the factor as per-plane outer products: no full
     // 4-D table and no table over both in-plane axes of a half-step

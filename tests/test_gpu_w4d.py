@@ -341,3 +341,41 @@ def test_r4p_matches_r4(dtype, monkeypatch):
     for name in OBS:
         assert rel_err(getattr(f1, name), getattr(f2, name)) < 1e-13, name
     assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < 1e-13
+
+
+def _notebook_windows(p):
+    """The reference notebooks' ambiguity windows (delta N != 1)."""
+    p.update(theta_x_amplitude=9.0, theta_y_amplitude=9.0, lambda_x_amplitude=9.0, lambda_y_amplitude=9.0)
+    return p
+
+
+def test_general_delta_fused_vs_oracle_32():
+    """General delta on a 32^4 grid: both half-steps in k_dense_half."""
+    p, c = config1(9, 32)
+    p = _notebook_windows(p)
+    init = lambda f, o: o.ho_ground(c[0], c[1], c[2], c[3], 1.0, 1.0, 1.0) / np.pi ** 2
+    f, Wo, obs = _run_both(p, init, 4)
+    for name in OBS:
+        assert rel_err(getattr(f, name), obs[name]) < 1e-12, name
+    assert rel_err(f.W_init_gpu.get(), Wo) < 1e-10
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-12), (np.complex64, 1e-4)])
+def test_general_delta_fused_matches_unfused_64(dtype, tol, monkeypatch):
+    """k_dense_half against the unfused FAFT passes on the notebook windows at 64^4."""
+    from configs import cat_xp
+    p, c = config2(10, 64)
+    p = _notebook_windows(p)
+    f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    monkeypatch.setenv("WIG_NO_DENSE_FUSED", "1")
+    f2 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    monkeypatch.delenv("WIG_NO_DENSE_FUSED")
+    W0 = cat_xp(f1._coords, c).astype(dtype)
+    for f in (f1, f2):
+        f.W_init_gpu.set(W0)
+        f.timeSteps = 3
+        f.fileName = None
+        f.Run()
+    for name in OBS:
+        assert rel_err(getattr(f1, name), getattr(f2, name)) < tol, name
+    assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < (1e-10 if tol < 1e-6 else 1e-3)
