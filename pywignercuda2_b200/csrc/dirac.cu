@@ -25,6 +25,9 @@
 #include "fft_smem.cuh"
 
 void* wig_dense_matrix(int n, double delta, int dtype, cudaStream_t st);
+int wig_r4_twiddles(void* tw, int dtype, cudaStream_t st);
+int wig_dplane64(void* const* slots, int nslots, int dtype, int kind, int fwd, double scale, const double* d_norm,
+                 const void* tw, cudaStream_t st);
 
 #define NSLOT 16
 
@@ -583,6 +586,7 @@ struct wigd_plan {
     int* counter;
     int* flag;
     int nblk;
+    void* tw64;              // twiddles of k_dplane_r4 (64^4 grids only)
 };
 
 static unsigned dgrid(long long n) {
@@ -596,6 +600,7 @@ static void free_dplan(wigd_plan* p) {
     cudaFree(p->tabs);
     cudaFree(p->partials);
     cudaFree(p->cur_norm);
+    cudaFree(p->tw64);
     delete p;
 }
 
@@ -685,6 +690,10 @@ extern "C" int wigd_plan_create(const wigd_desc* desc, wigd_plan** out) {
         const bool fast = (ns[a] == 16 || ns[a] == 32 || ns[a] == 64 || ns[a] == 128) &&
                           fabs(fabs(desc->delta[a]) * ns[a] - 1.0) < 1e-12;
         if (!fast && !wig_dense_matrix(ns[a], fabs(desc->delta[a]), desc->dtype, 0)) { free_dplan(p); return WIG_ERR_ALLOC; }
+    }
+    if (N0 == 64 && N1 == 64 && N2 == 64 && N3 == 64) {
+        if (cudaMalloc(&p->tw64, 64 * sizeof(double2)) != cudaSuccess) { free_dplan(p); return WIG_ERR_ALLOC; }
+        if (wig_r4_twiddles(p->tw64, desc->dtype, 0) != WIG_OK) { free_dplan(p); return WIG_ERR_CUDA; }
     }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { wig_set_cuda_error(e, "wigd_plan_create"); free_dplan(p); return WIG_ERR_CUDA; }
@@ -863,6 +872,11 @@ static int launch_dplane(wigd_plan* p, const Slots<C>& S, int nslots, double2 sc
     const int NB = KIND == 0 ? p->d.shape[3] : p->d.shape[2];
     const unsigned planes = KIND == 0 ? (unsigned)(p->d.shape[0] * p->d.shape[2]) : (unsigned)(p->d.shape[1] * p->d.shape[3]);
     dim3 grid(planes, nslots);
+    if (p->tw64 && !getenv("WIG_NO_DPLANE_R4")) {   // 64^4: radix-4 register transform
+        void* ptrs[NSLOT];
+        for (int k = 0; k < nslots; ++k) ptrs[k] = S.p[k];
+        return wig_dplane64(ptrs, nslots, p->d.dtype, KIND, FWD ? 1 : 0, sc.x, d_norm, p->tw64, st);
+    }
     constexpr int G = 32 / (int)sizeof(C);
 #define DCASE(a, b)                                                                              \
     if (NA == a && NB == b) {                                                                    \

@@ -495,6 +495,184 @@ template <class C>
 __global__ void k_make_r4_twiddles(C* tw) { r4::make_tw<C>(tw); }
 
 // ---------------------------------------------------------------------------
+// k_dplane_r4: the Wigner-Dirac component-plane transforms on 64^4 grids,
+//   value_out = scale * S * DFT2(S * value_in),  S = (-1)^(row + col),
+// the pair of centred FAFT calls for |delta| N = 1 that the reference's
+// Fourier_*_64_64_4x4_GPU wrappers make per component
+// (GPU_WignerDirac4D.py:1428-1596).
+//
+// One plane per CTA (blockIdx.x the plane, blockIdx.y the component slot),
+// in place.  The plane is read in natural order straight into layout L1 and
+// goes L1 -> L2 -> L3 like the forward half of k_r4 (conjugate kernels and
+// twiddles for the inverse direction: the same digit order with w^-1).
+// Each thread then holds the frequencies (kr, kc) = (r2 + 4 r1 + 16 i,
+// c2 + 4 c1 + 16 j) and stores them from registers: two exchanges per
+// transform and no staging.  S is constant over a thread's 16 points in L1
+// (parity of ar + ac) and in L3 (parity of r2 + c2), since the register
+// digits enter with weight 16.
+//   KIND 0: plane (i0, i2), rows axis 1 (stride 64^2), columns axis 3 (stride 1)
+//   KIND 1: plane (i1, i3), rows axis 0 (stride 64^3), columns axis 2 (stride 64);
+//           consecutive blocks are neighbouring i3, so the two (complex128)
+//           or four (complex64) planes of each 32-byte sector are read and
+//           written together and the sector is completed in L2.
+template <class C> struct PlaneSlots { C* p[16]; };
+
+template <class C, int KIND, bool FWD>
+__global__ void __launch_bounds__(r4::NT, (sizeof(C) == 16 ? 2 : 4))
+k_dplane_r4(PlaneSlots<C> S, const C* __restrict__ gtw, double2 scale, const double* __restrict__ d_norm) {
+    using namespace r4;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* s = reinterpret_cast<C*>(smraw);
+    C* tw = s + 64 * 64;
+    const int t = threadIdx.x, ac = t & 15, ar = t >> 4, pl = blockIdx.x;
+    const long long rs = KIND == 0 ? 64LL * 64 : 64LL * 64 * 64;
+    const long long cs = KIND == 0 ? 1 : 64;
+    const long long off = KIND == 0 ? (long long)(pl >> 6) * (64 * 64 * 64) + (long long)(pl & 63) * 64
+                                    : (long long)(pl >> 6) * (64 * 64) + (pl & 63);
+    C* g = S.p[blockIdx.y] + off;
+    C v[16];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[4 * i + j] = g[(ar + 16 * i) * rs + (ac + 16 * j) * cs];
+    if (t < 64) tw[t] = gtw[t];
+    double2 sc = scale;
+    if (d_norm) sc = zmul(sc, zinv(make_double2(d_norm[0], d_norm[1])));
+    const C cc = to_c<C>(sc);
+    if ((ar + ac) & 1) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = cneg(v[k]);
+    }
+    const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
+    __syncthreads();                                   // twiddles ready
+    pass<C, FWD>(v);
+    twiddle<C, FWD>(v, tw, ac, ar);
+    put(s, L1, v);
+    __syncthreads();
+    get(s, L2, v);
+    pass<C, FWD>(v);
+    twiddle<C, FWD>(v, tw, 4 * (t & 3), 4 * ((t >> 4) & 3));
+    __syncthreads();
+    put(s, L2, v);
+    __syncthreads();
+    get(s, L3, v);
+    pass<C, FWD>(v);
+    const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
+    const C ccs = ((r2 + c2) & 1) ? cneg(cc) : cc;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            g[(r2 + 4 * r1 + 16 * i) * rs + (c2 + 4 * c1 + 16 * j) * cs] = cmul(v[4 * i + j], ccs);
+}
+
+// k_dplane_r4t: the KIND 1 transform of k_dplane_r4 with the plane moved by
+// the tensor memory accelerator.  A (axis 0, axis 2) plane at fixed (i1, i3)
+// is 4096 points at a 1 KB stride, so per-thread loads and stores touch one
+// cache line per point.  Here one cp.async.bulk.tensor box per CTA brings
+// GP = 16 B / sizeof(C) neighbouring planes (i3 = GP m .. GP m + GP - 1: one
+// 16-byte piece of every row) into shared memory as [i0][i2][g], and one
+// tensor store writes the result back from the same buffer.  Thread group
+// g = t / 256 transforms plane g exactly as k_dplane_r4 does.
+// Map (innermost first, reals): (2 * 64, i2, i1, i0), box (2 GP, 64, 1, 64),
+// 64 KB per box for both dtypes; the box's x coordinate is 16 m bytes.
+// The load completes on an mbarrier whose wait is bounded: after the limit
+// the CTA writes NaN into its first plane (the next reduction reports a
+// non-finite norm), waits once more (bounded) and returns.
+template <class C> struct PlaneMaps { CUtensorMap m[16]; };
+
+namespace dpt {
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        ::"r"(r4t::sa(dst)), "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(r4t::sa(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3, const void* src) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];"
+                 ::"l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(r4t::sa(src))
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+}  // namespace dpt
+
+template <class C>
+constexpr int dplane_gp() { return 16 / (int)sizeof(C); }
+template <class C>
+constexpr size_t dplane_r4t_smem_bytes() { return 128 + 65536 + 64 * sizeof(C) + 16; }
+
+template <class C, bool FWD>
+__global__ void __launch_bounds__(r4::NT * dplane_gp<C>(), 2)
+k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, PlaneSlots<C> S, const C* __restrict__ gtw, double2 scale,
+             const double* __restrict__ d_norm) {
+    using namespace r4;
+    constexpr int GP = dplane_gp<C>();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* s = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+    C* tw = s + 4096 * GP;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tw + 64);
+    const int t = threadIdx.x & 255, grp = threadIdx.x >> 8, ac = t & 15, ar = t >> 4;
+    const int i1 = blockIdx.x / (64 / GP), m = blockIdx.x % (64 / GP);
+    const CUtensorMap* map = &maps.m[blockIdx.y];
+    if (threadIdx.x == 0) {
+        r4t::mbar_init(bar);
+        r4t::fence_async_smem();
+        r4t::mbar_expect_tx(bar, 65536);
+        dpt::tma_load_4d(s, map, 2 * GP * m, 0, i1, 0, bar);
+    }
+    if (threadIdx.x < 64) tw[threadIdx.x] = gtw[threadIdx.x];
+    double2 sc = scale;
+    if (d_norm) sc = zmul(sc, zinv(make_double2(d_norm[0], d_norm[1])));
+    const C cc = to_c<C>(sc);
+    __syncthreads();                                   // barrier initialised, twiddles ready
+    if (!r4t::mbar_wait_bounded(bar)) {
+        if (threadIdx.x == 0) {
+            typedef typename real_of<C>::type R;
+            S.p[blockIdx.y][(long long)i1 * 64 * 64 + GP * m].x = (R)__longlong_as_double(0x7ff8000000000000LL);
+        }
+        r4t::mbar_wait_bounded(bar);
+        return;
+    }
+    C v[16];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[4 * i + j] = s[((ar + 16 * i) * 64 + ac + 16 * j) * GP + grp];
+    if ((ar + ac) & 1) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = cneg(v[k]);
+    }
+    C* sg = s + 4096 * grp;                            // this group's exchange plane
+    const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
+    __syncthreads();                                   // the box has been read
+    pass<C, FWD>(v);
+    twiddle<C, FWD>(v, tw, ac, ar);
+    put(sg, L1, v);
+    __syncthreads();
+    get(sg, L2, v);
+    pass<C, FWD>(v);
+    twiddle<C, FWD>(v, tw, 4 * (t & 3), 4 * ((t >> 4) & 3));
+    __syncthreads();
+    put(sg, L2, v);
+    __syncthreads();
+    get(sg, L3, v);
+    pass<C, FWD>(v);
+    const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
+    const C ccs = ((r2 + c2) & 1) ? cneg(cc) : cc;
+    __syncthreads();                                   // every group's last exchange has been read
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            s[((r2 + 4 * r1 + 16 * i) * 64 + c2 + 4 * c1 + 16 * j) * GP + grp] = cmul(v[4 * i + j], ccs);
+    r4t::fence_async_smem();                           // generic-proxy writes visible to the tensor store
+    __syncthreads();
+    if (threadIdx.x == 0) dpt::tma_store_4d(map, 2 * GP * m, 0, i1, 0, s);
+}
+
+// ---------------------------------------------------------------------------
 // k_r4p: k_r4 as a persistent kernel that overlaps each plane's transforms
 // with the load of its next plane.
 //

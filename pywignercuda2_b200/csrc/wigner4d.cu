@@ -1528,6 +1528,98 @@ extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     return WIG_OK;
 }
 
+// ---- 64 x 64 component-plane transforms for the Wigner-Dirac plan ----------
+// (dirac.cu calls these; the kernels share the k_r4 machinery in r4.cuh)
+int wig_r4_twiddles(void* tw, int dtype, cudaStream_t st) {
+    if (dtype == WIG_C128) k_make_r4_twiddles<double2><<<1, 64, 0, st>>>((double2*)tw);
+    else k_make_r4_twiddles<float2><<<1, 64, 0, st>>>((float2*)tw);
+    WIG_LAUNCHED("k_make_r4_twiddles");
+    return WIG_OK;
+}
+
+template <class C, int KIND, bool FWD>
+static int launch_dplane_r4(void* const* slots, int nslots, const void* tw, double scale, const double* d_norm,
+                            cudaStream_t st) {
+    PlaneSlots<C> S;
+    for (int k = 0; k < 16; ++k) S.p[k] = k < nslots ? (C*)slots[k] : nullptr;
+    auto kern = k_dplane_r4<C, KIND, FWD>;
+    const size_t sm = sizeof(C) * (64 * 64 + 64);
+    WIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<dim3(64 * 64, nslots), r4::NT, sm, st>>>(S, (const C*)tw, make_double2(scale, 0.0), d_norm);
+    WIG_LAUNCHED("k_dplane_r4");
+    return WIG_OK;
+}
+
+// 4-D view of one 64^4 component for k_dplane_r4t: (2 * 64 reals, i2, i1, i0),
+// box (2 GP reals = 16 bytes, 64, 1, 64).
+template <class C>
+static int encode_dplane_map(CUtensorMap* m, const void* base) {
+    constexpr cuuint64_t E = sizeof(C);
+    const cuuint64_t dims[4] = {128, 64, 64, 64};
+    const cuuint64_t strides[3] = {64 * E, 64 * 64 * E, 64 * 64 * 64 * E};
+    const cuuint32_t box[4] = {(cuuint32_t)(2 * dplane_gp<C>()), 64, 1, 64};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    EncodeTiledFn enc = encode_tiled_fn();
+    if (!enc) {
+        snprintf(wig_last_error_buffer(), 256, "cuTensorMapEncodeTiled is not available from the driver");
+        return WIG_ERR_CUDA;
+    }
+    const CUresult r = enc(m, E == 16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                           const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(wig_last_error_buffer(), 256, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return WIG_ERR_CUDA;
+    }
+    return WIG_OK;
+}
+
+template <class C, bool FWD>
+static int launch_dplane_r4t(void* const* slots, int nslots, const void* tw, double scale, const double* d_norm,
+                             cudaStream_t st) {
+    PlaneMaps<C> maps;
+    PlaneSlots<C> S;
+    memset(&maps, 0, sizeof(maps));
+    for (int k = 0; k < 16; ++k) S.p[k] = k < nslots ? (C*)slots[k] : nullptr;
+    for (int k = 0; k < nslots; ++k) {
+        int r;
+        if ((r = encode_dplane_map<C>(&maps.m[k], slots[k]))) return r;
+    }
+    constexpr int GP = dplane_gp<C>();
+    auto kern = k_dplane_r4t<C, FWD>;
+    const size_t sm = dplane_r4t_smem_bytes<C>();
+    WIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<dim3(64 * 64 / GP, nslots), r4::NT * GP, sm, st>>>(maps, S, (const C*)tw, make_double2(scale, 0.0),
+                                                              d_norm);
+    WIG_LAUNCHED("k_dplane_r4t");
+    return WIG_OK;
+}
+
+// kind 0: axes (1, 3), kind 1: axes (0, 2) of a 64^4 component; fwd: exp(-i ...)
+int wig_dplane64(void* const* slots, int nslots, int dtype, int kind, int fwd, double scale, const double* d_norm,
+                 const void* tw, cudaStream_t st) {
+    if (nslots < 1 || nslots > 16 || !tw) return WIG_ERR_INVALID_ARG;
+    for (int k = 0; k < nslots; ++k)
+        if (!slots[k] || (reinterpret_cast<uintptr_t>(slots[k]) & 15)) return WIG_ERR_INVALID_ARG;
+    if (kind == 1 && !getenv("WIG_NO_DPLANE_TMA")) {
+        if (dtype == WIG_C128) return fwd ? launch_dplane_r4t<double2, true>(slots, nslots, tw, scale, d_norm, st)
+                                          : launch_dplane_r4t<double2, false>(slots, nslots, tw, scale, d_norm, st);
+        return fwd ? launch_dplane_r4t<float2, true>(slots, nslots, tw, scale, d_norm, st)
+                   : launch_dplane_r4t<float2, false>(slots, nslots, tw, scale, d_norm, st);
+    }
+    if (dtype == WIG_C128) {
+        if (kind == 0) return fwd ? launch_dplane_r4<double2, 0, true>(slots, nslots, tw, scale, d_norm, st)
+                                  : launch_dplane_r4<double2, 0, false>(slots, nslots, tw, scale, d_norm, st);
+        return fwd ? launch_dplane_r4<double2, 1, true>(slots, nslots, tw, scale, d_norm, st)
+                   : launch_dplane_r4<double2, 1, false>(slots, nslots, tw, scale, d_norm, st);
+    }
+    if (kind == 0) return fwd ? launch_dplane_r4<float2, 0, true>(slots, nslots, tw, scale, d_norm, st)
+                              : launch_dplane_r4<float2, 0, false>(slots, nslots, tw, scale, d_norm, st);
+    return fwd ? launch_dplane_r4<float2, 1, true>(slots, nslots, tw, scale, d_norm, st)
+               : launch_dplane_r4<float2, 1, false>(slots, nslots, tw, scale, d_norm, st);
+}
+
 extern "C" long long wig4d_plan_device_bytes(const wig4d_plan* p) {
     if (!p) return -1;
     const long long N0 = p->shape[0], N1 = p->shape[1], N2 = p->shape[2], N3 = p->shape[3];

@@ -173,3 +173,75 @@ def test_golden_x_notebook_on_gpu():
     f.Run()
     for k in range(3):
         assert abs(f.norms[k].real - g["run_norms"][k]) < 1e-10 * g["run_norms"][k], k
+
+
+def _centred_dft2(X, fwd):
+    """S DFT2(S X), S = (-1)^(row + col); the inverse unnormalised."""
+    n0, n1 = X.shape
+    S = (-1.0) ** (np.arange(n0)[:, None] + np.arange(n1)[None, :])
+    F = np.fft.fft2(S * X) if fwd else np.fft.ifft2(S * X) * (n0 * n1)
+    return S * F
+
+
+@pytest.mark.parametrize("variant", ["tma", "plain"])
+@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-13), (np.complex64, 5e-6)])
+def test_dplane_r4_64(dtype, tol, variant, monkeypatch):
+    """The 64^4 component-plane transforms of all four Dirac wrappers
+    (k_dplane_r4; for P <-> Theta k_dplane_r4t, or k_dplane_r4 with
+    WIG_NO_DPLANE_TMA): against NumPy's 2-D FFT on sampled planes, and
+    against the generic plane kernels (k_dplane / k_dplane_g) on two whole
+    components."""
+    if variant == "plain":
+        monkeypatch.setenv("WIG_NO_DPLANE_TMA", "1")
+    p = small(64, fast=True)
+    f = make_frame(GPU_WignerDirac4D, p, complex_dtype=dtype)
+    tdt = torch.complex128 if dtype == np.complex128 else torch.complex64
+    g = torch.Generator(device="cuda").manual_seed(11)
+    base = [torch.randn(f.shape, dtype=tdt, device="cuda", generator=g) for _ in range(2)]
+    s = float(64 ** 4)
+    post = [1.0 / s, 100.0 / np.sqrt(s), 1.0 / s, 100.0 / np.sqrt(s)]
+    d = [f.dp_y, f.dy, f.dp_x, f.dx]
+    rng = np.random.default_rng(4)
+    for which in range(4):
+        got = [b.clone() for b in base]
+        f._transform(got, which)
+        monkeypatch.setenv("WIG_NO_DPLANE_R4", "1")
+        ref = [b.clone() for b in base]
+        f._transform(ref, which)
+        monkeypatch.delenv("WIG_NO_DPLANE_R4")
+        torch.cuda.synchronize()
+        for a, b in zip(got, ref):
+            assert ((a - b).abs().max() / b.abs().max()).item() < tol, which
+        ax = (1, 3) if which < 2 else (0, 2)
+        sc = post[which] * (2 * 64 * d[ax[0]]) * (2 * 64 * d[ax[1]])
+        src, out = base[0].cpu().numpy().astype(np.complex128), got[0].cpu().numpy()
+        for _ in range(3):
+            f0, f1 = (int(v) for v in rng.integers(0, 64, size=2))
+            if which < 2:
+                X, Y = src[f0, :, f1, :], out[f0, :, f1, :]
+            else:
+                X, Y = src[:, f0, :, f1], out[:, f0, :, f1]
+            E = sc * _centred_dft2(X, which in (0, 2))
+            assert np.max(np.abs(Y - E)) / np.max(np.abs(E)) < tol, which
+
+
+def test_run_64_matches_generic_planes(monkeypatch):
+    """Two Run() iterations at 64^4 (delta = 1/N): the k_dplane_r4 /
+    k_dplane_r4t transforms against the generic plane kernels."""
+    p = small(64, fast=True)
+    f = make_frame(GPU_WignerDirac4D, p, bound_p=15.0)
+    f.fileName = None
+    f.timeSteps = 2
+    out = []
+    for env in (None, "1"):
+        if env:
+            monkeypatch.setenv("WIG_NO_DPLANE_R4", env)
+        Ws = all_w(f)
+        for W in Ws:                      # the initial state writes four components only
+            W.tensor.zero_()
+        f.WignerDiracGaussian_ParticleUp_GPU(*Ws, 0.5, 0.1, 0.3, -0.2, 2.2, 1.9)
+        f._Fourier_Theta_To_P_64_64_4x4_GPU(*Ws)
+        f.Run()
+        out.append((np.array(f.norms), np.array(f.energyKinetic), np.array(f.average_x), f.W11.get(), f.W14.get()))
+    for a, b in zip(out[0], out[1]):
+        assert rel_err(a, b) < 1e-11
