@@ -71,15 +71,28 @@ struct DParams {
     const double* mxp[4];                          // boundary_xp factors per axis
     const double* mp[4];                           // boundary_p factors per axis
     int arank;                                     // rank of the A1..A3 tables
-    const double* atab;                            // [3][2][R][N3*N2 + N1*N0]
+    const double* atab;                            // [3][2][R][N2*N3 + N1*N0], u part [itx][ix]
     const double* obs_xy;                          // [7][N1][N3]
+    int pow2, s3, s32, s321;                       // all sizes powers of two: shifts of axes 2, 1, 0
 };
 
-__device__ __forceinline__ void decode(long long i, const DParams& P, int& i0, int& i1, int& i2, int& i3) {
-    i3 = (int)(i % P.n3);
-    i2 = (int)((i / P.n3) % P.n2);
-    i1 = (int)((i / ((long long)P.n3 * P.n2)) % P.n1);
-    i0 = (int)(i / ((long long)P.n3 * P.n2 * P.n1));
+// Point index -> (i0, i1, i2, i3) in 32-bit arithmetic (plans hold fewer
+// than 2^31 points): shifts and masks for power-of-two sizes, else three
+// unsigned divisions.
+__device__ __forceinline__ void decode(long long li, const DParams& P, int& i0, int& i1, int& i2, int& i3) {
+    const unsigned i = (unsigned)li;
+    if (P.pow2) {
+        i3 = (int)(i & (unsigned)(P.n3 - 1));
+        i2 = (int)((i >> P.s3) & (unsigned)(P.n2 - 1));
+        i1 = (int)((i >> P.s32) & (unsigned)(P.n1 - 1));
+        i0 = (int)(i >> P.s321);
+        return;
+    }
+    const unsigned q3 = i / (unsigned)P.n3, q2 = q3 / (unsigned)P.n2, q1 = q2 / (unsigned)P.n1;
+    i3 = (int)(i - q3 * (unsigned)P.n3);
+    i2 = (int)(q3 - q2 * (unsigned)P.n2);
+    i1 = (int)(q2 - q1 * (unsigned)P.n1);
+    i0 = (int)q1;
 }
 
 // ---------------------------------------------------------------------------
@@ -104,7 +117,17 @@ __device__ __forceinline__ M4 spin_matrix(double2 a, double2 b, double s, double
     return m;
 }
 
-// w <- L * w * R (4 x 4), w row-major w[4*a + b]
+// Structural non-zeros of the matrices (bit 4 r + c set for entry (r, c)):
+// spin_matrix and the KvN potential propagator have two per row, the Dirac
+// potential propagator three (no (0,1), (1,0), (2,3), (3,2)).
+constexpr unsigned SPIN_NZ = (1u << 0) | (1u << 3) | (1u << 5) | (1u << 6) | (1u << 9) | (1u << 10) |
+                             (1u << 12) | (1u << 15);
+constexpr unsigned DPOT_NZ = 0xffffu & ~((1u << 1) | (1u << 4) | (1u << 11) | (1u << 14));
+
+// w <- L * w * R (4 x 4), w row-major w[4*a + b]; entries outside NZ are
+// zero and their products are skipped (each sum runs over the non-zero
+// entries in increasing k, as the dense product adds them).
+template <unsigned NZL, unsigned NZR>
 __device__ __forceinline__ void sandwich(const M4& L, double2 (&w)[16], const M4& R) {
     double2 t[16];
 #pragma unroll
@@ -113,7 +136,8 @@ __device__ __forceinline__ void sandwich(const M4& L, double2 (&w)[16], const M4
         for (int b = 0; b < 4; ++b) {
             double2 s = make_double2(0.0, 0.0);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) s = zadd(s, zmul(L.a[a][k], w[4 * k + b]));
+            for (int k = 0; k < 4; ++k)
+                if ((NZL >> (4 * a + k)) & 1u) s = zadd(s, zmul(L.a[a][k], w[4 * k + b]));
             t[4 * a + b] = s;
         }
 #pragma unroll
@@ -122,7 +146,8 @@ __device__ __forceinline__ void sandwich(const M4& L, double2 (&w)[16], const M4
         for (int b = 0; b < 4; ++b) {
             double2 s = make_double2(0.0, 0.0);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) s = zadd(s, zmul(t[4 * a + k], R.a[k][b]));
+            for (int k = 0; k < 4; ++k)
+                if ((NZR >> (4 * k + b)) & 1u) s = zadd(s, zmul(t[4 * a + k], R.a[k][b]));
             w[4 * a + b] = s;
         }
 }
@@ -195,7 +220,7 @@ __device__ __forceinline__ double a_field(const DParams& P, int k, int side, int
     double acc = 0.0;
     for (int r = 0; r < P.arank; ++r) {
         const double* f = base + r * (nu + nv);
-        acc = fma(f[(long long)ix * P.n2 + itx], f[nu + (long long)iy * P.n0 + ity], acc);
+        acc = fma(f[(long long)itx * P.n3 + ix], f[nu + (long long)iy * P.n0 + ity], acc);
     }
     return acc;
 }
@@ -249,7 +274,7 @@ __global__ void k_dreal(Slots<C> S, long long n) {
 // projector (sign != 0, first) and kinetic sandwich (kin != 0) on the
 // (lambda, p) grid: axis 0 p_y, 1 lambda_y, 2 p_x, 3 lambda_x
 template <class C>
-__global__ void k_dkinetic(Slots<C> S, DParams P, int sign, int kin, double dlx, double dly) {
+__global__ void __launch_bounds__(256, 2) k_dkinetic(Slots<C> S, DParams P, int sign, int kin, double dlx, double dly) {
     const long long n = (long long)P.n0 * P.n1 * P.n2 * P.n3;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         int i0, i1, i2, i3;
@@ -275,7 +300,7 @@ __global__ void k_dkinetic(Slots<C> S, DParams P, int sign, int kin, double dlx,
             const M4 L = proj(pxp, pyp), R = proj(pxm, pym);
 #pragma unroll
             for (int k = 0; k < 16; ++k) w[k] = zscale(w[k], 0.25);
-            sandwich(L, w, R);
+            sandwich<SPIN_NZ, SPIN_NZ>(L, w, R);
         }
         if (kin) {          // WD4D:392-481
             double pxp, pyp, pxm, pym;
@@ -288,7 +313,7 @@ __global__ void k_dkinetic(Slots<C> S, DParams P, int sign, int kin, double dlx,
             kin_entries(pxp, pyp, P.mass, P.dt, P, a, b);
             kin_entries(pxm, pym, P.mass, -P.dt, P, cc, d);
             const M4 L = spin_matrix(a, b, -1.0, zconj(a)), R = spin_matrix(cc, d, -1.0, zconj(cc));
-            sandwich(L, w, R);
+            sandwich<SPIN_NZ, SPIN_NZ>(L, w, R);
             const double r = exp(-P.dt * dlx * lx * lx - P.dt * dly * ly * ly);
 #pragma unroll
             for (int k = 0; k < 16; ++k) w[k] = zscale(w[k], r);
@@ -299,7 +324,7 @@ __global__ void k_dkinetic(Slots<C> S, DParams P, int sign, int kin, double dlx,
 
 // potential sandwich on the (x, theta) grid: axis 0 theta_y, 1 y, 2 theta_x, 3 x
 template <class C>
-__global__ void k_dpotential(Slots<C> S, DParams P, DFactors<C> phase) {
+__global__ void __launch_bounds__(128, 3) k_dpotential(Slots<C> S, DParams P, DFactors<C> phase) {
     const long long n = (long long)P.n0 * P.n1 * P.n2 * P.n3;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         int i0, i1, i2, i3;
@@ -312,7 +337,8 @@ __global__ void k_dpotential(Slots<C> S, DParams P, DFactors<C> phase) {
         const double A3p = a_field(P, 2, 1, i3, i2, i1, i0);
         const M4 UL = pot_matrix(A1m, A2m, A3m, P.dt, false, P);
         const M4 UR = pot_matrix(A1p, A2p, A3p, P.kvn ? P.dt : -P.dt, true, P);
-        sandwich(UL, w, UR);
+        if (P.kvn) sandwich<SPIN_NZ, SPIN_NZ>(UL, w, UR);
+        else sandwich<DPOT_NZ, DPOT_NZ>(UL, w, UR);
         const double2 ev = dfactor_at(phase, i0, i1, i2, i3, i);
 #pragma unroll
         for (int k = 0; k < 16; ++k) w[k] = zmul(w[k], ev);
@@ -589,8 +615,8 @@ struct wigd_plan {
     void* tw64;              // twiddles of k_dplane_r4 (64^4 grids only)
 };
 
-static unsigned dgrid(long long n) {
-    long long b = (n + 255) / 256, cap = (long long)wig_num_sms() * 8;
+static unsigned dgrid(long long n, int threads = 256, int per_sm = 8) {
+    long long b = (n + threads - 1) / threads, cap = (long long)wig_num_sms() * per_sm;
     return (unsigned)(b < cap ? (b > 0 ? b : 1) : cap);
 }
 
@@ -620,6 +646,7 @@ extern "C" int wigd_plan_create(const wigd_desc* desc, wigd_plan** out) {
     p->d = *desc;
     const int N0 = desc->shape[0], N1 = desc->shape[1], N2 = desc->shape[2], N3 = desc->shape[3];
     p->npts = (long long)N0 * N1 * N2 * N3;
+    if (p->npts >= (1LL << 31)) { delete p; return WIG_ERR_UNSUPPORTED; }   // 32-bit point indices
     p->esz = desc->dtype == WIG_C128 ? 16 : 8;
     const int ns[4] = {N0, N1, N2, N3};
     // ---- float64 tables in one allocation ----
@@ -634,7 +661,17 @@ extern "C" int wigd_plan_create(const wigd_desc* desc, wigd_plan** out) {
         }
     }
     const long long off_a = h.size();
-    if (desc->a_rank > 0) h.insert(h.end(), desc->a_tabs, desc->a_tabs + 6LL * desc->a_rank * (nu + nv));
+    if (desc->a_rank > 0) {
+        // the u part of each table, given as [ix][itx], is stored as [itx][ix] so
+        // that neighbouring x points read neighbouring words
+        h.insert(h.end(), desc->a_tabs, desc->a_tabs + 6LL * desc->a_rank * (nu + nv));
+        for (long long b = 0; b < 6LL * desc->a_rank; ++b) {
+            const double* src = desc->a_tabs + b * (nu + nv);
+            double* dst = h.data() + off_a + b * (nu + nv);
+            for (int ix = 0; ix < N3; ++ix)
+                for (int itx = 0; itx < N2; ++itx) dst[(long long)itx * N3 + ix] = src[(long long)ix * N2 + itx];
+        }
+    }
     const long long off_o = h.size();
     h.insert(h.end(), desc->obs_xy, desc->obs_xy + 7LL * N1 * N3);
     if (cudaMalloc(&p->dmem, h.size() * sizeof(double)) != cudaSuccess) { free_dplan(p); return WIG_ERR_ALLOC; }
@@ -642,6 +679,9 @@ extern "C" int wigd_plan_create(const wigd_desc* desc, wigd_plan** out) {
     double* D = p->dmem;
     DParams& P = p->P;
     P.n0 = N0; P.n1 = N1; P.n2 = N2; P.n3 = N3;
+    auto lg = [](int n) { int l = 0; while ((1 << l) < n) ++l; return (1 << l) == n ? l : -1; };
+    P.pow2 = lg(N0) >= 0 && lg(N1) >= 0 && lg(N2) >= 0 && lg(N3) >= 0;
+    if (P.pow2) { P.s3 = lg(N3); P.s32 = P.s3 + lg(N2); P.s321 = P.s32 + lg(N1); }
     P.kvn = desc->kvn;
     P.c = desc->c; P.hbar = desc->hbar; P.mass = desc->mass; P.dt = desc->dt; P.m_pot = desc->m_pot;
     P.cpy = D + offs[0][0]; P.cy = D + offs[1][0]; P.cpx = D + offs[2][0]; P.cx = D + offs[3][0];
@@ -826,7 +866,7 @@ static int potential_impl(wigd_plan* p, void* const* slots, cudaStream_t st) {
     Slots<C> S;
     int r = make_slots(slots, S, true);
     if (r) return r;
-    k_dpotential<C><<<dgrid(p->npts), 256, 0, st>>>(S, p->P, phase_set<C>(p));
+    k_dpotential<C><<<dgrid(p->npts, 128, 12), 128, 0, st>>>(S, p->P, phase_set<C>(p));
     WIG_LAUNCHED("k_dpotential");
     return WIG_OK;
 }

@@ -74,10 +74,15 @@ def all_w(f):
     return [getattr(f, n) for n in NAMES]
 
 
+@pytest.mark.parametrize("n", [16, 48])
 @pytest.mark.parametrize("kvn", [False, True])
 @pytest.mark.parametrize("fast", [False, True])
-def test_elementwise_and_transforms(kvn, fast):
-    p = small(16, kvn, fast)
+def test_elementwise_and_transforms(kvn, fast, n):
+    """Every kernel once against the oracle; n = 48 takes the point decoding
+    for sizes that are not powers of two (radix windows only, to stay small)."""
+    if n == 48 and not fast:
+        pytest.skip("48^4 runs with delta = 1/N windows only")
+    p = small(n, kvn, fast)
     f, o = pair(p, kvn)
     set_state(f, o)
     f.Fourier_X_To_Lambda_64_64_4x4_GPU(*all_w(f))
