@@ -400,52 +400,52 @@ __global__ void k_dinit(Slots<C> S, DParams P, int kind, double a0, double a1, d
 //  0,1 sum trace (complex)   2 x tr  3 p_x tr  4 x^2 tr  5 p_x^2 tr  6 y tr  7 p_y tr
 //  8 y^2 tr  9 p_y^2 tr  10 alpha1  11 alpha2  12 x alpha1  13 y alpha2  14 kinetic energy
 //  15 potential energy  16 D1A0  17 D1A1  18 D1A2  19 unused
-template <class C>
-__global__ void __launch_bounds__(256) k_dreduce(Slots<C> S, DParams P, double* __restrict__ partials) {
-    __shared__ double sm[DSUM * 8];
-    double a[DSUM];
-#pragma unroll
-    for (int k = 0; k < DSUM; ++k) a[k] = 0.0;
-    const long long n = (long long)P.n0 * P.n1 * P.n2 * P.n3;
+// Components the sums read (W11 W13 W14 W22 W23 W24 W31 W32 W33 W41 W42 W44).
+constexpr unsigned RED_SLOTS = 0xffffu & ~((1u << 1) | (1u << 4) | (1u << 11) | (1u << 14));
+
+// One point's contributions to the DSUM sums; w row-major W11..W44.
+__device__ __forceinline__ void dreduce_point(const DParams& P, int i0, int i1, int i2, int i3,
+                                              const double2 (&w)[16], double (&a)[DSUM]) {
     const long long nxy = (long long)P.n1 * P.n3;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        int i0, i1, i2, i3;
-        decode(i, P, i0, i1, i2, i3);
-        const double x = P.cx[i3], px = P.cpx[i2], y = P.cy[i1], py = P.cpy[i0];
-        const double2 W11 = to_d2(S.p[0][i]), W22 = to_d2(S.p[5][i]), W33 = to_d2(S.p[10][i]), W44 = to_d2(S.p[15][i]);
-        const double2 W14 = to_d2(S.p[3][i]), W41 = to_d2(S.p[12][i]), W23 = to_d2(S.p[6][i]), W32 = to_d2(S.p[9][i]);
-        const double2 W13 = to_d2(S.p[2][i]), W24 = to_d2(S.p[7][i]), W31 = to_d2(S.p[8][i]), W42 = to_d2(S.p[13][i]);
-        const double trr = W11.x + W22.x + W33.x + W44.x, tri = W11.y + W22.y + W33.y + W44.y;
-        const double a1 = W14.x + W41.x + W23.x + W32.x;           // Re(W14+W41+W23+W32)
-        const double a2 = -(W14.y - W41.y + W32.y - W23.y);        // -Im(W14-W41+W32-W23)
-        const double mterm = W11.x + W22.x - W33.x - W44.x;
-        const long long ixy = (long long)i1 * P.n3 + i3;
-        const double A0 = P.obs_xy[ixy], A1 = P.obs_xy[nxy + ixy], A2 = P.obs_xy[2 * nxy + ixy];
-        const double A3 = P.obs_xy[3 * nxy + ixy], D10 = P.obs_xy[4 * nxy + ixy];
-        const double D11 = P.obs_xy[5 * nxy + ixy], D12 = P.obs_xy[6 * nxy + ixy];
-        const double c = P.c;
-        a[0] += trr; a[1] += tri;
-        a[2] = fma(x, trr, a[2]); a[3] = fma(px, trr, a[3]);
-        a[4] = fma(x * x, trr, a[4]); a[5] = fma(px * px, trr, a[5]);
-        a[6] = fma(y, trr, a[6]); a[7] = fma(py, trr, a[7]);
-        a[8] = fma(y * y, trr, a[8]); a[9] = fma(py * py, trr, a[9]);
-        a[10] += a1; a[11] += a2;
-        a[12] = fma(x, a1, a[12]); a[13] = fma(y, a2, a[13]);
-        // c p_x Re(W14+W41+W32+W23) - c p_y Im(W14-W41+W32-W23) + m c^2 Re(W11+W22-W33-W44)
-        a[14] += c * px * a1 + c * py * a2 + P.mass * c * c * mterm;
-        if (P.kvn) {   // KvN:1107-1109, 1137
-            const double k2 = W14.y - W41.y - W23.y + W32.y;
-            a[15] += A1 * c * a1 - A2 * c * k2 + c * A0 * trr;
-            a[18] += c * D12 * (W14.x - W41.x - W23.x + W32.x);
-        } else {       // WD4D:1309-1312, 1340
-            const double e2 = -W14.y + W23.y - W32.y + W41.y;
-            const double e3 = -W13.x + W24.x - W31.x + W42.x;
-            a[15] += A1 * c * (-a1) - A2 * c * e2 + A3 * c * e3 + c * A0 * trr;
-            a[18] += -D12 * c * e2;
-        }
-        a[16] += c * D10 * trr;
-        a[17] += c * D11 * a1;
+    const double x = P.cx[i3], px = P.cpx[i2], y = P.cy[i1], py = P.cpy[i0];
+    const double2 W11 = w[0], W22 = w[5], W33 = w[10], W44 = w[15];
+    const double2 W14 = w[3], W41 = w[12], W23 = w[6], W32 = w[9];
+    const double2 W13 = w[2], W24 = w[7], W31 = w[8], W42 = w[13];
+    const double trr = W11.x + W22.x + W33.x + W44.x, tri = W11.y + W22.y + W33.y + W44.y;
+    const double a1 = W14.x + W41.x + W23.x + W32.x;           // Re(W14+W41+W23+W32)
+    const double a2 = -(W14.y - W41.y + W32.y - W23.y);        // -Im(W14-W41+W32-W23)
+    const double mterm = W11.x + W22.x - W33.x - W44.x;
+    const long long ixy = (long long)i1 * P.n3 + i3;
+    const double A0 = P.obs_xy[ixy], A1 = P.obs_xy[nxy + ixy], A2 = P.obs_xy[2 * nxy + ixy];
+    const double A3 = P.obs_xy[3 * nxy + ixy], D10 = P.obs_xy[4 * nxy + ixy];
+    const double D11 = P.obs_xy[5 * nxy + ixy], D12 = P.obs_xy[6 * nxy + ixy];
+    const double c = P.c;
+    a[0] += trr; a[1] += tri;
+    a[2] = fma(x, trr, a[2]); a[3] = fma(px, trr, a[3]);
+    a[4] = fma(x * x, trr, a[4]); a[5] = fma(px * px, trr, a[5]);
+    a[6] = fma(y, trr, a[6]); a[7] = fma(py, trr, a[7]);
+    a[8] = fma(y * y, trr, a[8]); a[9] = fma(py * py, trr, a[9]);
+    a[10] += a1; a[11] += a2;
+    a[12] = fma(x, a1, a[12]); a[13] = fma(y, a2, a[13]);
+    // c p_x Re(W14+W41+W32+W23) - c p_y Im(W14-W41+W32-W23) + m c^2 Re(W11+W22-W33-W44)
+    a[14] += c * px * a1 + c * py * a2 + P.mass * c * c * mterm;
+    if (P.kvn) {   // KvN:1107-1109, 1137
+        const double k2 = W14.y - W41.y - W23.y + W32.y;
+        a[15] += A1 * c * a1 - A2 * c * k2 + c * A0 * trr;
+        a[18] += c * D12 * (W14.x - W41.x - W23.x + W32.x);
+    } else {       // WD4D:1309-1312, 1340
+        const double e2 = -W14.y + W23.y - W32.y + W41.y;
+        const double e3 = -W13.x + W24.x - W31.x + W42.x;
+        a[15] += A1 * c * (-a1) - A2 * c * e2 + A3 * c * e3 + c * A0 * trr;
+        a[18] += -D12 * c * e2;
     }
+    a[16] += c * D10 * trr;
+    a[17] += c * D11 * a1;
+}
+
+// The block's sums -> one partial row (256 threads).
+__device__ __forceinline__ void dreduce_block(double (&a)[DSUM], double* __restrict__ partials) {
+    __shared__ double sm[DSUM * 8];
 #pragma unroll
     for (int k = 0; k < DSUM; ++k) {
 #pragma unroll
@@ -460,6 +460,51 @@ __global__ void __launch_bounds__(256) k_dreduce(Slots<C> S, DParams P, double* 
         for (int k = 0; k < 8; ++k) t += sm[k * DSUM + threadIdx.x];
         partials[(long long)blockIdx.x * DSUM + threadIdx.x] = t;
     }
+}
+
+template <class C>
+__global__ void __launch_bounds__(256) k_dreduce(Slots<C> S, DParams P, double* __restrict__ partials) {
+    double a[DSUM];
+#pragma unroll
+    for (int k = 0; k < DSUM; ++k) a[k] = 0.0;
+    const long long n = (long long)P.n0 * P.n1 * P.n2 * P.n3;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int i0, i1, i2, i3;
+        decode(i, P, i0, i1, i2, i3);
+        double2 w[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) w[k] = ((RED_SLOTS >> k) & 1u) ? to_d2(S.p[k][i]) : make_double2(0.0, 0.0);
+        dreduce_point(P, i0, i1, i2, i3, w, a);
+    }
+    dreduce_block(a, partials);
+}
+
+// The Run() loop's first three passes in one: boundary_xp (k_dmask kind 1),
+// Real_GPU of the diagonal (k_dreal) and the sums (k_dreduce) of the result.
+// Needs distinct component pointers; the sums see the stored (rounded)
+// values, as k_dreduce would.
+template <class C>
+__global__ void __launch_bounds__(256, 2) k_dmask_real_reduce(Slots<C> S, DParams P, double* __restrict__ partials) {
+    double a[DSUM];
+#pragma unroll
+    for (int k = 0; k < DSUM; ++k) a[k] = 0.0;
+    const long long n = (long long)P.n0 * P.n1 * P.n2 * P.n3;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int i0, i1, i2, i3;
+        decode(i, P, i0, i1, i2, i3);
+        const double r = P.mxp[2][i2] * P.mxp[0][i0] * P.mxp[3][i3] * P.mxp[1][i1];
+        double2 w[16];
+        load16(S, i, w);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            C v = to_c<C>(zscale(w[k], r));
+            if (k == 0 || k == 5 || k == 10 || k == 15) v.y = 0;
+            S.p[k][i] = v;
+            w[k] = to_d2(v);
+        }
+        dreduce_point(P, i0, i1, i2, i3, w, a);
+    }
+    dreduce_block(a, partials);
 }
 
 // out: [norm_re, norm_im, 17 observables] = WIGD_NOBS values.  When divide,
@@ -998,12 +1043,23 @@ extern "C" int wigd_transform(wigd_plan* p, void* const* slots, int nslots, int 
 template <class C>
 static int run_impl(wigd_plan* p, void* const* slots, int iterations, int filter, double* hist, cudaStream_t st) {
     int r;
+    Slots<C> S;
+    if ((r = make_slots(slots, S, false))) return r;
+    const bool fused_mrr = getenv("WIG_NO_DFUSE") == nullptr;
     WIG_CUDA(cudaMemsetAsync(p->counter, 0, 2 * sizeof(int), st));
     for (int it = 0; it < iterations; ++it) {
         // boundary_xp, Real, trace norm + observables of the normalised state
-        if ((r = mask_impl<C>(p, slots, 1, st))) return r;
-        if ((r = real_impl<C>(p, slots, st))) return r;
-        if ((r = reduce_impl<C>(p, slots, hist, 1, p->counter, iterations, st))) return r;
+        if (fused_mrr) {
+            k_dmask_real_reduce<C><<<p->nblk, 256, 0, st>>>(S, p->P, p->partials);
+            WIG_LAUNCHED("k_dmask_real_reduce");
+            k_dfinalize<<<1, 32 * DSUM, 0, st>>>(p->partials, p->nblk, p->d.dv_norm, p->d.dv_obs, 1, hist,
+                                                 p->counter, iterations, p->cur_norm, p->flag);
+            WIG_LAUNCHED("k_dfinalize");
+        } else {
+            if ((r = mask_impl<C>(p, slots, 1, st))) return r;
+            if ((r = real_impl<C>(p, slots, st))) return r;
+            if ((r = reduce_impl<C>(p, slots, hist, 1, p->counter, iterations, st))) return r;
+        }
         // X -> Lambda with the 1/norm folded in
         if ((r = transform_impl<C>(p, slots, NSLOT, 0, p->cur_norm, st))) return r;
         if ((r = kinetic_impl<C>(p, slots, filter ? 1 : 0, 1, st))) return r;

@@ -250,3 +250,22 @@ def test_run_64_matches_generic_planes(monkeypatch):
         out.append((np.array(f.norms), np.array(f.energyKinetic), np.array(f.average_x), f.W11.get(), f.W14.get()))
     for a, b in zip(out[0], out[1]):
         assert rel_err(a, b) < 1e-11
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_fused_mask_real_reduce_bitwise(dtype, monkeypatch):
+    """The device loop's fused boundary/Real/sums pass (k_dmask_real_reduce)
+    gives the same bits as the three separate kernels (WIG_NO_DFUSE)."""
+    p = small(16, fast=True)
+    out = []
+    for env in (None, "1"):
+        if env:
+            monkeypatch.setenv("WIG_NO_DFUSE", env)
+        f, o = pair(p, False, alias_w21=False, bound_p=15.0, complex_dtype=dtype)
+        set_state(f, o, 5)
+        f.timeSteps = 3
+        f.fileName = None
+        f.Run()
+        out.append((np.array(f.norms), np.array(f.energyKinetic), np.array(f.average_x), f.W11.get(), f.W23.get()))
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
