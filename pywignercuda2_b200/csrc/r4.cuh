@@ -672,6 +672,97 @@ k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, PlaneSlots<C> S, const C
     if (threadIdx.x == 0) dpt::tma_store_4d(map, 2 * GP * m, 0, i1, 0, s);
 }
 
+// k_dplane_r4c: k_dplane_r4t with 32-byte box rows, half the rows per box.
+// A cluster of two CTAs takes the GPB = 32 B / sizeof(C) neighbouring planes
+// of one 32-byte piece (i3 = GPB m .. GPB m + GPB - 1).  CTA q loads the rows
+// i0 = 32 q .. 32 q + 31 of all GPB planes (box (2 GPB reals, 64, 1, 32),
+// 64 KB, stored as [i0 - 32 q][i2][plane]) and transforms the GP = GPB / 2
+// planes q GP + g, reading the other half of their rows from the partner's
+// box through distributed shared memory.  The results are staged back into
+// the two boxes the same way, and each CTA writes its box with one tensor
+// store.  Rows of a thread's points: ar + 16 i, so registers i = 0, 1 live in
+// CTA 0's box and i = 2, 3 in CTA 1's, for the load and for the staging.
+// A bounded wait that runs out does not leave early: both CTAs pass every
+// cluster barrier, the CTA skips its store, writes NaN into its first plane
+// and waits once more (bounded) for its copy.
+template <class C, bool FWD>
+__global__ void __launch_bounds__(r4::NT * dplane_gp<C>(), 2)
+k_dplane_r4c(const __grid_constant__ PlaneMaps<C> maps, PlaneSlots<C> S, const C* __restrict__ gtw, double2 scale,
+             const double* __restrict__ d_norm) {
+    using namespace r4;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    constexpr int GP = dplane_gp<C>(), GPB = 2 * GP;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* s = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+    C* tw = s + 4096 * GP;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tw + 64);
+    const int t = threadIdx.x & 255, grp = threadIdx.x >> 8, ac = t & 15, ar = t >> 4;
+    const int q = (int)cl.block_rank(), pair = blockIdx.x >> 1;
+    const int i1 = pair / (64 / GPB), m = pair % (64 / GPB), pg = q * GP + grp;
+    const CUtensorMap* map = &maps.m[blockIdx.y];
+    if (threadIdx.x == 0) {
+        r4t::mbar_init(bar);
+        r4t::fence_async_smem();
+        r4t::mbar_expect_tx(bar, 65536);
+        dpt::tma_load_4d(s, map, 2 * GPB * m, 0, i1, 32 * q, bar);
+    }
+    if (threadIdx.x < 64) tw[threadIdx.x] = gtw[threadIdx.x];
+    double2 sc = scale;
+    if (d_norm) sc = zmul(sc, zinv(make_double2(d_norm[0], d_norm[1])));
+    const C cc = to_c<C>(sc);
+    C* box[2] = {cl.map_shared_rank(s, 0), cl.map_shared_rank(s, 1)};
+    __syncthreads();                                   // barrier initialised, twiddles ready
+    const bool ok = r4t::mbar_wait_bounded(bar);
+    cl.sync();                                         // both boxes in place
+    C v[16];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            v[4 * i + j] = box[i >> 1][((ar + 16 * (i & 1)) * 64 + ac + 16 * j) * GPB + pg];
+    if ((ar + ac) & 1) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = cneg(v[k]);
+    }
+    C* sg = s + 4096 * grp;                            // this group's exchange plane
+    const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
+    cl.sync();                                         // both boxes have been read
+    pass<C, FWD>(v);
+    twiddle<C, FWD>(v, tw, ac, ar);
+    put(sg, L1, v);
+    __syncthreads();
+    get(sg, L2, v);
+    pass<C, FWD>(v);
+    twiddle<C, FWD>(v, tw, 4 * (t & 3), 4 * ((t >> 4) & 3));
+    __syncthreads();
+    put(sg, L2, v);
+    __syncthreads();
+    get(sg, L3, v);
+    pass<C, FWD>(v);
+    const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
+    const C ccs = ((r2 + c2) & 1) ? cneg(cc) : cc;
+    cl.sync();                                         // every exchange plane of both CTAs has been read
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            box[i >> 1][((r2 + 4 * r1 + 16 * (i & 1)) * 64 + c2 + 4 * c1 + 16 * j) * GPB + pg] =
+                cmul(v[4 * i + j], ccs);
+    asm volatile("fence.proxy.async;" ::: "memory");   // staged writes (local and remote) visible to the store
+    cl.sync();
+    if (threadIdx.x == 0) {
+        if (ok) {
+            dpt::tma_store_4d(map, 2 * GPB * m, 0, i1, 32 * q, s);
+        } else {
+            typedef typename real_of<C>::type R;
+            S.p[blockIdx.y][(long long)i1 * 64 * 64 + GPB * m + q * GP].x =
+                (R)__longlong_as_double(0x7ff8000000000000LL);
+            r4t::mbar_wait_bounded(bar);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // k_r4p: k_r4 as a persistent kernel that overlaps each plane's transforms
 // with the load of its next plane.

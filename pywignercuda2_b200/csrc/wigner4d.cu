@@ -1550,14 +1550,16 @@ static int launch_dplane_r4(void* const* slots, int nslots, const void* tw, doub
     return WIG_OK;
 }
 
-// 4-D view of one 64^4 component for k_dplane_r4t: (2 * 64 reals, i2, i1, i0),
-// box (2 GP reals = 16 bytes, 64, 1, 64).
+// 4-D view of one 64^4 component for k_dplane_r4t / k_dplane_r4c:
+// (2 * 64 reals, i2, i1, i0); box (reals, 64, 1, rows): (2 GP reals = 16
+// bytes, 64, 1, 64) for k_dplane_r4t, (4 GP reals = 32 bytes, 64, 1, 32) for
+// k_dplane_r4c.
 template <class C>
-static int encode_dplane_map(CUtensorMap* m, const void* base) {
+static int encode_dplane_map(CUtensorMap* m, const void* base, int reals, int rows) {
     constexpr cuuint64_t E = sizeof(C);
     const cuuint64_t dims[4] = {128, 64, 64, 64};
     const cuuint64_t strides[3] = {64 * E, 64 * 64 * E, 64 * 64 * 64 * E};
-    const cuuint32_t box[4] = {(cuuint32_t)(2 * dplane_gp<C>()), 64, 1, 64};
+    const cuuint32_t box[4] = {(cuuint32_t)reals, 64, 1, (cuuint32_t)rows};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     EncodeTiledFn enc = encode_tiled_fn();
     if (!enc) {
@@ -1584,7 +1586,7 @@ static int launch_dplane_r4t(void* const* slots, int nslots, const void* tw, dou
     for (int k = 0; k < 16; ++k) S.p[k] = k < nslots ? (C*)slots[k] : nullptr;
     for (int k = 0; k < nslots; ++k) {
         int r;
-        if ((r = encode_dplane_map<C>(&maps.m[k], slots[k]))) return r;
+        if ((r = encode_dplane_map<C>(&maps.m[k], slots[k], 2 * dplane_gp<C>(), 64))) return r;
     }
     constexpr int GP = dplane_gp<C>();
     auto kern = k_dplane_r4t<C, FWD>;
@@ -1596,12 +1598,49 @@ static int launch_dplane_r4t(void* const* slots, int nslots, const void* tw, dou
     return WIG_OK;
 }
 
+template <class C, bool FWD>
+static int launch_dplane_r4c(void* const* slots, int nslots, const void* tw, double scale, const double* d_norm,
+                             cudaStream_t st) {
+    PlaneMaps<C> maps;
+    PlaneSlots<C> S;
+    memset(&maps, 0, sizeof(maps));
+    for (int k = 0; k < 16; ++k) S.p[k] = k < nslots ? (C*)slots[k] : nullptr;
+    constexpr int GP = dplane_gp<C>();
+    for (int k = 0; k < nslots; ++k) {
+        int r;
+        if ((r = encode_dplane_map<C>(&maps.m[k], slots[k], 4 * GP, 32))) return r;
+    }
+    auto kern = k_dplane_r4c<C, FWD>;
+    const size_t sm = dplane_r4t_smem_bytes<C>();
+    WIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * 64 * 64 / (2 * GP), nslots);
+    cfg.blockDim = dim3(r4::NT * GP);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    WIG_CUDA(cudaLaunchKernelEx(&cfg, kern, maps, S, (const C*)tw, make_double2(scale, 0.0), d_norm));
+    return WIG_OK;
+}
+
 // kind 0: axes (1, 3), kind 1: axes (0, 2) of a 64^4 component; fwd: exp(-i ...)
 int wig_dplane64(void* const* slots, int nslots, int dtype, int kind, int fwd, double scale, const double* d_norm,
                  const void* tw, cudaStream_t st) {
     if (nslots < 1 || nslots > 16 || !tw) return WIG_ERR_INVALID_ARG;
     for (int k = 0; k < nslots; ++k)
         if (!slots[k] || (reinterpret_cast<uintptr_t>(slots[k]) & 15)) return WIG_ERR_INVALID_ARG;
+    if (kind == 1 && !getenv("WIG_NO_DPLANE_TMA") && getenv("WIG_DPLANE_CLUSTER")) {
+        if (dtype == WIG_C128) return fwd ? launch_dplane_r4c<double2, true>(slots, nslots, tw, scale, d_norm, st)
+                                          : launch_dplane_r4c<double2, false>(slots, nslots, tw, scale, d_norm, st);
+        return fwd ? launch_dplane_r4c<float2, true>(slots, nslots, tw, scale, d_norm, st)
+                   : launch_dplane_r4c<float2, false>(slots, nslots, tw, scale, d_norm, st);
+    }
     if (kind == 1 && !getenv("WIG_NO_DPLANE_TMA")) {
         if (dtype == WIG_C128) return fwd ? launch_dplane_r4t<double2, true>(slots, nslots, tw, scale, d_norm, st)
                                           : launch_dplane_r4t<double2, false>(slots, nslots, tw, scale, d_norm, st);

@@ -188,16 +188,18 @@ def _centred_dft2(X, fwd):
     return S * F
 
 
-@pytest.mark.parametrize("variant", ["tma", "plain"])
+@pytest.mark.parametrize("variant", ["tma", "cluster", "plain"])
 @pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-13), (np.complex64, 5e-6)])
 def test_dplane_r4_64(dtype, tol, variant, monkeypatch):
     """The 64^4 component-plane transforms of all four Dirac wrappers
-    (k_dplane_r4; for P <-> Theta k_dplane_r4t, or k_dplane_r4 with
-    WIG_NO_DPLANE_TMA): against NumPy's 2-D FFT on sampled planes, and
+    (k_dplane_r4; for P <-> Theta k_dplane_r4t, k_dplane_r4c with
+    WIG_DPLANE_CLUSTER, or k_dplane_r4 with WIG_NO_DPLANE_TMA): against NumPy's 2-D FFT on sampled planes, and
     against the generic plane kernels (k_dplane / k_dplane_g) on two whole
     components."""
     if variant == "plain":
         monkeypatch.setenv("WIG_NO_DPLANE_TMA", "1")
+    if variant == "cluster":
+        monkeypatch.setenv("WIG_DPLANE_CLUSTER", "1")
     p = small(64, fast=True)
     f = make_frame(GPU_WignerDirac4D, p, complex_dtype=dtype)
     tdt = torch.complex128 if dtype == np.complex128 else torch.complex64
