@@ -185,17 +185,13 @@ def bench_batched(steps):
             "speedup_vs_one_at_a_time_plain": ms_plain / ms_batch}
 
 
-def bench_dirac(steps):
+def _dirac_frame(steps, complex_dtype=np.complex128):
     """The Wigner-Dirac workload: 64^4 grid x 16 components (4.3 GB in
     complex128), V = 0.3 (x^2 + y^2), symmetric-gauge field B in U[0.1, 0.5],
-    D_lambda = 0.005, dt = 0.002, delta = 1/N windows, positive-energy Gaussian
-    spinor.  Steps/s of Run() in the reference's call sequence (the W21 alias,
-    the default) and of the fused device loop (alias off), CUDA events."""
+    D_lambda = 0.005, dt = 0.002, delta = 1/N windows."""
     import math
-    import torch
     from frames import make_frame
     from pywignercuda2_b200 import GPU_WignerDirac4D
-    from pywignercuda2_b200.dirac4d import NAMES
     rng = np.random.default_rng(5000)
     B = float(rng.uniform(0.1, 0.5))
     x0, y0 = (float(v) for v in rng.uniform(-2, 2, size=2))
@@ -210,11 +206,59 @@ def bench_dirac(steps):
                   potential_3_String="0.", D_1_potential_0_String="0.6*x", D_1_potential_1_String="0.",
                   D_1_potential_2_String="%r/2." % B, D_theta_x=0.0, D_theta_y=0.0,
                   D_lambda_x=0.005, D_lambda_y=0.005)
+    f = make_frame(GPU_WignerDirac4D, params, complex_dtype=complex_dtype)
+    f.fileName = None
+    return f, B, (x0, y0)
+
+
+def dirac_passes(f, reps=5):
+    """Milliseconds of each pass of one Dirac Run() iteration on the frame's
+    state (CUDA events around `reps` launches of each)."""
+    import torch
+    from pywignercuda2_b200 import _lib
+    from pywignercuda2_b200.device import stream_ptr
+    from pywignercuda2_b200.dirac4d import NAMES
+    Ws = [getattr(f, k) for k in NAMES]
+    slots = f._slots(Ws)
+    obs = torch.zeros(64, dtype=torch.float64, device="cuda")
+    plan = f._plan
+    stages = [
+        ("boundary", lambda: _lib.call("wigd_mask", plan, slots, 1, stream_ptr())),
+        ("real", lambda: _lib.call("wigd_real_diag", plan, slots, stream_ptr())),
+        ("sums", lambda: _lib.call("wigd_reduce", plan, slots, obs.data_ptr(), 0, stream_ptr())),
+        ("x_to_lambda", lambda: f._transform(Ws, 0)),
+        ("kinetic", lambda: _lib.call("wigd_kinetic", plan, slots, 0, 1, stream_ptr())),
+        ("lambda_to_x", lambda: f._transform(Ws, 1)),
+        ("p_to_theta", lambda: f._transform(Ws, 2)),
+        ("potential", lambda: _lib.call("wigd_potential", plan, slots, stream_ptr())),
+        ("theta_to_p", lambda: f._transform(Ws, 3)),
+    ]
+    out = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for name, fn in stages:
+        fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1) / reps
+    return out
+
+
+def bench_dirac(steps):
+    """The Wigner-Dirac workload (`_dirac_frame`) from a positive-energy
+    Gaussian spinor.  Steps/s of Run() in the reference's call sequence (the
+    W21 alias, the default) and of the fused device loop (alias off), CUDA
+    events, and the milliseconds of each pass."""
+    import torch
+    from pywignercuda2_b200.dirac4d import NAMES
+    f, B, (x0, y0) = _dirac_frame(steps)
+    n = 64
     out = {"workload": "WignerDirac4D 64^4 x 16 components, complex128, B=%.3f, dt=0.002" % B,
            "state_bytes": 16 * n ** 4 * 16, "steps": steps}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f = make_frame(GPU_WignerDirac4D, params)
-    f.fileName = None
     Ws = [getattr(f, k) for k in NAMES]
     for alias in (True, False):
         f.alias_w21 = alias
@@ -236,6 +280,7 @@ def bench_dirac(steps):
         out[key] = {"steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps,
                     "hbm_gbs_per_sweep_equivalent": 2 * out["state_bytes"] / (ms / steps / 1e3) / 1e9,
                     "finite": bool(np.all(np.isfinite(f.energyKinetic)))}
+    out["pass_ms"] = dirac_passes(f)
     del f
     return out
 
@@ -271,10 +316,20 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--no-dirac", action="store_true", help="skip the Wigner-Dirac line")
     ap.add_argument("--dirac-steps", type=int, default=20)
+    ap.add_argument("--dirac-passes", choices=["c128", "c64"],
+                    help="only time each pass of one Wigner-Dirac iteration in this dtype and exit")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
+    if args.dirac_passes:
+        from pywignercuda2_b200.dirac4d import NAMES
+        f, _, (x0, y0) = _dirac_frame(2, np.complex64 if args.dirac_passes == "c64" else np.complex128)
+        Ws = [getattr(f, k) for k in NAMES]
+        f.WignerDiracGaussian_ParticleUp_GPU(*Ws, 0.0, 0.0, x0, y0, 1.0, 1.0)
+        f._Fourier_Theta_To_P_64_64_4x4_GPU(*Ws)
+        print(json.dumps({"dirac_pass_ms": dirac_passes(f), "dtype": args.dirac_passes}), flush=True)
+        return 0
 
     import torch
     import torch.distributed as dist
