@@ -74,6 +74,7 @@ struct DParams {
     const double* atab;                            // [3][2][R][N2*N3 + N1*N0], u part [itx][ix]
     const double* obs_xy;                          // [7][N1][N3]
     int pow2, s3, s32, s321;                       // all sizes powers of two: shifts of axes 2, 1, 0
+    int a3zero;                                    // A3 vanishes on both Bopp sides (rank tables)
 };
 
 // Point index -> (i0, i1, i2, i3) in 32-bit arithmetic (plans hold fewer
@@ -203,6 +204,7 @@ __device__ __forceinline__ M4 pot_matrix(double A1, double A2, double A3, double
     u.a[1][2] = make_double2(A2 * sf, -A1 * sf);
     u.a[2][1] = make_double2(-A2 * sf, -A1 * sf);
     u.a[3][0] = make_double2(-A2 * sf, A1 * sf);
+    if (P.a3zero) return u;                        // sin(A3 c dt) = 0: the four entries below vanish
     const double s3 = sin(A3 * c * dt);
     u.a[0][2] = make_double2(0.0, s3);
     u.a[1][3] = make_double2(0.0, -s3);
@@ -332,12 +334,12 @@ __global__ void __launch_bounds__(128, 3) k_dpotential(Slots<C> S, DParams P, DF
         double2 w[16];
         load16(S, i, w);
         const double A1m = a_field(P, 0, 0, i3, i2, i1, i0), A2m = a_field(P, 1, 0, i3, i2, i1, i0);
-        const double A3m = a_field(P, 2, 0, i3, i2, i1, i0);
+        const double A3m = P.a3zero ? 0.0 : a_field(P, 2, 0, i3, i2, i1, i0);
         const double A1p = a_field(P, 0, 1, i3, i2, i1, i0), A2p = a_field(P, 1, 1, i3, i2, i1, i0);
-        const double A3p = a_field(P, 2, 1, i3, i2, i1, i0);
+        const double A3p = P.a3zero ? 0.0 : a_field(P, 2, 1, i3, i2, i1, i0);
         const M4 UL = pot_matrix(A1m, A2m, A3m, P.dt, false, P);
         const M4 UR = pot_matrix(A1p, A2p, A3p, P.kvn ? P.dt : -P.dt, true, P);
-        if (P.kvn) sandwich<SPIN_NZ, SPIN_NZ>(UL, w, UR);
+        if (P.kvn || P.a3zero) sandwich<SPIN_NZ, SPIN_NZ>(UL, w, UR);
         else sandwich<DPOT_NZ, DPOT_NZ>(UL, w, UR);
         const double2 ev = dfactor_at(phase, i0, i1, i2, i3, i);
 #pragma unroll
@@ -734,6 +736,17 @@ extern "C" int wigd_plan_create(const wigd_desc* desc, wigd_plan** out) {
     for (int a = 0; a < 4; ++a) { P.mxp[a] = D + offs[a][2]; P.mp[a] = D + offs[a][3]; }
     P.arank = desc->a_rank;
     P.atab = D + off_a;
+    // A3 = sum_r u_r(x, theta_x) v_r(y, theta_y) on both sides: zero when every
+    // rank term has an all-zero factor (or there is no rank term)
+    P.a3zero = 1;
+    for (int side = 0; side < 2 && P.a3zero; ++side)
+        for (int r = 0; r < desc->a_rank; ++r) {
+            const double* f = desc->a_tabs + ((long long)(2 * 2 + side) * desc->a_rank + r) * (nu + nv);
+            bool uz = true, vz = true;
+            for (long long e = 0; e < nu && uz; ++e) uz = f[e] == 0.0;
+            for (long long e = 0; e < nv && vz; ++e) vz = f[nu + e] == 0.0;
+            if (!uz && !vz) { P.a3zero = 0; break; }
+        }
     P.obs_xy = D + off_o;
     // ---- A0 phase factor tables ----
     auto tab_elems = [&](const wig_factor& f) -> long long {

@@ -271,3 +271,24 @@ def test_fused_mask_real_reduce_bitwise(dtype, monkeypatch):
         out.append((np.array(f.norms), np.array(f.energyKinetic), np.array(f.average_x), f.W11.get(), f.W23.get()))
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b)
+
+
+def test_run_parity_a3_zero():
+    """A3 = 0 (the symmetric-gauge configs): the potential pass skips the
+    sin(A3 c dt) entries and uses the two-per-row sandwich; against the oracle."""
+    p = small(16, False, True, potential_3_String="0.")
+    f, o = pair(p, False, alias_w21=False, bound_p=15.0)
+    set_state(f, o, 7)
+    f.timeSteps = 3
+    f.fileName = None
+    f.Run()
+    Ws = o.pointers(False)
+    norms, obs = [], []
+    for _ in range(4):
+        n, ob = o.run_iteration(Ws, filter_particle=False, bound_p=15.0)
+        norms.append(n)
+        obs.append(ob)
+    assert rel_err(f.norms, np.array(norms)) < 1e-12
+    for name in ["average_x", "energyKinetic", "energyPotential"]:
+        assert rel_err(getattr(f, name), np.array([ob[name] for ob in obs])) < 1e-11, name
+    assert err16(comps(f), o.W) < 1e-11
