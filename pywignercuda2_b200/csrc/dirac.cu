@@ -241,29 +241,59 @@ __device__ __forceinline__ void store16(const Slots<C>& S, long long i, const do
 // ---------------------------------------------------------------------------
 // Elementwise kernels
 // ---------------------------------------------------------------------------
-// kind 1: boundary_xp (mxp), kind 2: boundary_p (mp).  Slot by slot
-// read-modify-write, like the reference's statements W11[i] = r*W11[i]; ...
+// The distinct component pointers of a slot list with how often each occurs
+// (the reference's Run() binds W21 to W22, so a pointer can occur twice).
 template <class C>
-__global__ void k_dmask(Slots<C> S, DParams P, int kind) {
+struct USlots {
+    C* p[NSLOT];
+    int mult[NSLOT];
+    int n;
+};
+
+// kind 1: boundary_xp (mxp), kind 2: boundary_p (mp).  The reference's
+// statements W11[i] = r*W11[i]; ... run slot by slot, so a pointer that
+// occurs m times is scaled m times; here each distinct pointer is loaded
+// once, scaled m times with the storage rounding between, and stored once.
+template <class C>
+__global__ void __launch_bounds__(256) k_dmask(USlots<C> U, DParams P, int kind) {
     const long long n = (long long)P.n0 * P.n1 * P.n2 * P.n3;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         int i0, i1, i2, i3;
         decode(i, P, i0, i1, i2, i3);
-        const double* const* m = kind == 1 ? P.mxp : P.mp;
-        const double r = m[2][i2] * m[0][i0] * m[3][i3] * m[1][i1];
-        for (int k = 0; k < 16; ++k) {
-            const double2 v = to_d2(S.p[k][i]);
-            S.p[k][i] = to_c<C>(zscale(v, r));
-        }
+        const double r = kind == 1 ? P.mxp[2][i2] * P.mxp[0][i0] * P.mxp[3][i3] * P.mxp[1][i1]
+                                   : P.mp[2][i2] * P.mp[0][i0] * P.mp[3][i3] * P.mp[1][i1];
+        C w[NSLOT];
+#pragma unroll
+        for (int u = 0; u < NSLOT; ++u)
+            if (u < U.n) w[u] = U.p[u][i];
+#pragma unroll
+        for (int u = 0; u < NSLOT; ++u)
+            if (u < U.n) {
+                C v = w[u];
+                for (int k = 0; k < U.mult[u]; ++k) v = to_c<C>(zscale(to_d2(v), r));
+                U.p[u][i] = v;
+            }
     }
 }
 
-// W[slot] /= *d_norm slot by slot (Normalize_4x4_GPU, WD4D:1366-1388)
+// W[slot] /= *d_norm slot by slot (Normalize_4x4_GPU, WD4D:1366-1388), over
+// the distinct pointers as k_dmask does
 template <class C>
-__global__ void k_ddivide(Slots<C> S, long long n, const double* d_norm) {
+__global__ void __launch_bounds__(256) k_ddivide(USlots<C> U, long long n, const double* d_norm) {
     const double2 inv = zinv(make_double2(d_norm[0], d_norm[1]));
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        for (int k = 0; k < 16; ++k) S.p[k][i] = to_c<C>(zmul(to_d2(S.p[k][i]), inv));
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        C w[NSLOT];
+#pragma unroll
+        for (int u = 0; u < NSLOT; ++u)
+            if (u < U.n) w[u] = U.p[u][i];
+#pragma unroll
+        for (int u = 0; u < NSLOT; ++u)
+            if (u < U.n) {
+                C v = w[u];
+                for (int k = 0; k < U.mult[u]; ++k) v = to_c<C>(zmul(to_d2(v), inv));
+                U.p[u][i] = v;
+            }
+    }
 }
 
 template <class C>
@@ -820,6 +850,23 @@ static int make_slots(void* const* slots, Slots<C>& S, bool allow_alias) {
     return WIG_OK;
 }
 
+template <class C>
+static USlots<C> unique_slots(const Slots<C>& S) {
+    USlots<C> U;
+    U.n = 0;
+    for (int k = 0; k < NSLOT; ++k) {
+        U.p[k] = nullptr;
+        U.mult[k] = 0;
+    }
+    for (int k = 0; k < NSLOT; ++k) {
+        int u = 0;
+        while (u < U.n && U.p[u] != S.p[k]) ++u;
+        if (u == U.n) U.p[U.n++] = S.p[k];
+        ++U.mult[u];
+    }
+    return U;
+}
+
 #define DISPATCH(p, body_c128, body_c64) \
     ((p)->d.dtype == WIG_C128 ? (body_c128) : (body_c64))
 
@@ -828,7 +875,7 @@ static int mask_impl(wigd_plan* p, void* const* slots, int kind, cudaStream_t st
     Slots<C> S;
     int r = make_slots(slots, S, true);
     if (r) return r;
-    k_dmask<C><<<dgrid(p->npts), 256, 0, st>>>(S, p->P, kind);
+    k_dmask<C><<<dgrid(p->npts), 256, 0, st>>>(unique_slots(S), p->P, kind);
     WIG_LAUNCHED("k_dmask");
     return WIG_OK;
 }
@@ -870,7 +917,7 @@ static int divide_impl(wigd_plan* p, void* const* slots, const double* d_norm, c
     Slots<C> S;
     int r = make_slots(slots, S, true);
     if (r) return r;
-    k_ddivide<C><<<dgrid(p->npts), 256, 0, st>>>(S, p->npts, d_norm);
+    k_ddivide<C><<<dgrid(p->npts), 256, 0, st>>>(unique_slots(S), p->npts, d_norm);
     WIG_LAUNCHED("k_ddivide");
     return WIG_OK;
 }
