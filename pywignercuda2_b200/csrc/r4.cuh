@@ -140,10 +140,17 @@ constexpr size_t r4_smem_bytes() { return sizeof(C) * (64 * 64 + 64) + sizeof(do
 // CL: launched as clusters of the IL planes f1 = IL m .. IL m + IL - 1 that
 // share each destination sector; the stores then go through distributed
 // shared memory so that every 32-byte sector is written whole (see the end).
-template <class C, bool KIN, bool CL>
+// PART: 0 the whole half-step; 1 its first half (load, forward transform,
+// factor), which stores the plane's frequencies from the L3 registers to
+// mid[plane][kr][kc] (whole lines); 2 its second half, which loads them back
+// into L3 and runs the inverse transform and the stores (and reductions).
+// The two halves move the state twice but each CTA does half the work per
+// byte, so loads and transforms of resident CTAs overlap better.
+template <class C, bool KIN, bool CL, int PART = 0>
 __global__ void __launch_bounds__(r4::NT, (sizeof(C) == 16 ? 2 : 4))
 k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__ PV, const C* __restrict__ gtw,
-     double2 scale, const double* __restrict__ d_norm, ObsTabs ob, double* __restrict__ partials) {
+     double2 scale, const double* __restrict__ d_norm, ObsTabs ob, double* __restrict__ partials,
+     C* __restrict__ mid) {
     using namespace r4;
     constexpr int IL = Il<C>::v, NQ = 64 / IL;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -152,8 +159,15 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
     double2* pvs = reinterpret_cast<double2*>(tw + 64);         // this plane's factor vectors
     const int t = threadIdx.x, pl = blockIdx.x, f0 = pl >> 6, f1 = pl & 63;
     const int ac = t & 15, ar = t >> 4;
+    // mid offset of register (i, j) in L3: kr = r2 + 4 r1 + 16 i, kc = c2 + 4 c1 + 16 j
+    const long long moff = (long long)pl * 4096 + ((t >> 6) + 4 * ((t >> 4) & 3)) * 64 + ((t >> 2) & 3) + 4 * (t & 3);
     C v[16];
-    {
+    if (PART == 2) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[4 * i + j] = mid[moff + i * 16 * 64 + j * 16];
+    } else {
         const C* g = src + ((((long long)ar * NQ + ac / IL) * 64 + f0) * 64 + f1) * IL + (ac % IL);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
@@ -162,11 +176,12 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
                 v[4 * i + j] = g[(long long)i * (16LL * 64 * 64 * 64) + (long long)j * (16LL * 64 * 64)];
     }
     if (t < 64) tw[t] = gtw[t];
-    if (t < 128) pvs[t] = __ldg(PV + (long long)pl * 128 + t);
+    if (PART != 2 && t < 128) pvs[t] = __ldg(PV + (long long)pl * 128 + t);
     double2 cc = scale;
     if (KIN && d_norm) cc = zmul(cc, zinv(make_double2(d_norm[0], d_norm[1])));
     const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
     __syncthreads();                                           // twiddles and factor vectors ready
+    if (PART != 2) {
     // ---- forward
     pass<C, true>(v);
     twiddle<C, true>(v, tw, ac, ar);
@@ -192,6 +207,14 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
 #pragma unroll
             for (int j = 0; j < 4; ++j) factor_mul(v[4 * i + j], a, b[j]);
         }
+    }
+    }  // PART != 2
+    if (PART == 1) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) mid[moff + i * 16 * 64 + j * 16] = v[4 * i + j];
+        return;
     }
     // ---- inverse
     pass<C, false>(v);

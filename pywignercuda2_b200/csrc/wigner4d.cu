@@ -997,6 +997,8 @@ struct wig4d_plan {
     bool r4t;                      // complex128 64^4 Run(): k_r4 with TMA plane loads (k_r4t)
     bool r4_cluster;               // k_r4 launched as clusters with full-sector stores
     bool r4p;                      // persistent k_r4p (next plane prefetched by cp.async)
+    bool r4split;                  // each k_r4 half-step as two launches (PART 1, 2) through mid
+    void* mid;                     // k_r4 split: the planes' frequencies between the two launches
     int dense_n;                   // > 0: general-delta half-steps fused (k_dense_half, N^4 grids)
     const void* dmat[4];           // FAFT matrices per axis (|delta|), when dense_n > 0
     int r4p_grid;                  // its CTAs: SMs x resident CTAs, a multiple of the cluster size
@@ -1195,6 +1197,7 @@ static void free_plan(wig4d_plan* p) {
     cudaFree(p->partials);
     cudaFree(p->cur_norm);
     cudaFree(p->pingpong);
+    cudaFree(p->mid);
     cudaFree(p->pv);
     cudaFree(p->tw64);
     cudaFree(p->fold);
@@ -1469,6 +1472,8 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             if (cudaMalloc(&p->tw64, 64 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
             if (cudaMalloc(&p->fold, FOLD_BLOCKS * NSUM * sizeof(double)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
             p->r4p = kern && strcmp(kern, "r4p") == 0;
+            p->r4split = !p->r4p && getenv("WIG_R4_SPLIT") != nullptr;
+            if (p->r4split && cudaMalloc(&p->mid, (size_t)p->npts * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
             if (p->r4p) {
                 const int psm = (int)(desc->dtype == WIG_C128 ? r4p_smem_bytes<double2>() : r4p_smem_bytes<float2>());
                 const int il = desc->dtype == WIG_C128 ? 2 : 4;
@@ -1493,11 +1498,23 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
                 cudaFuncSetAttribute(k_r4<double2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
                 cudaFuncSetAttribute(k_r4<double2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
                 cudaFuncSetAttribute(k_r4<double2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<double2, true, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<double2, false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<double2, true, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<double2, false, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<double2, true, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<double2, false, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
             } else {
                 cudaFuncSetAttribute(k_r4<float2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
                 cudaFuncSetAttribute(k_r4<float2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
                 cudaFuncSetAttribute(k_r4<float2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
                 cudaFuncSetAttribute(k_r4<float2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<float2, true, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<float2, false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<float2, true, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<float2, false, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<float2, true, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+                cudaFuncSetAttribute(k_r4<float2, false, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
             }
         }
         // the persistent kernels write one NSUM row per CTA
@@ -1664,7 +1681,7 @@ extern "C" long long wig4d_plan_device_bytes(const wig4d_plan* p) {
     const long long N0 = p->shape[0], N1 = p->shape[1], N2 = p->shape[2], N3 = p->shape[3];
     const long long esz = p->dtype == WIG_C128 ? 16 : 8;
     return p->tab_bytes + 8 * (N0 + N1 + N2 + N3 + N0 * N2 + N1 * N3) + 8LL * N1 * N3 * NPART + 32 +
-           (p->pingpong ? p->npts * esz : 0);
+           (p->pingpong ? p->npts * esz : 0) + (p->mid ? p->npts * esz : 0);
 }
 
 extern "C" int wig4d_kinetic(wig4d_plan* p, void* W, const double* d_norm, void* stream) {
@@ -1829,7 +1846,7 @@ static cudaError_t launch_r4(bool cluster, unsigned grid, size_t sm, cudaStream_
                              const double2* pv, const C* tw, double2 scale, const double* d_norm, ObsTabs ob,
                              double* partials) {
     if (!cluster) {
-        k_r4<C, KIN, false><<<grid, r4::NT, sm, st>>>(src, dst, pv, tw, scale, d_norm, ob, partials);
+        k_r4<C, KIN, false><<<grid, r4::NT, sm, st>>>(src, dst, pv, tw, scale, d_norm, ob, partials, nullptr);
         return cudaGetLastError();
     }
     cudaLaunchConfig_t cfg = {};
@@ -1844,7 +1861,36 @@ static cudaError_t launch_r4(bool cluster, unsigned grid, size_t sm, cudaStream_
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_r4<C, KIN, true>, src, dst, pv, tw, scale, d_norm, ob, partials);
+    return cudaLaunchKernelEx(&cfg, k_r4<C, KIN, true>, src, dst, pv, tw, scale, d_norm, ob, partials, (C*)nullptr);
+}
+
+// k_r4 as two launches: the first half (no clusters; whole-line stores to
+// mid), then the second half with the cluster stores of launch_r4.
+template <class C, bool KIN>
+static cudaError_t launch_r4_split(bool cluster, unsigned grid, size_t sm, cudaStream_t st, const C* src, C* dst,
+                                   const double2* pv, const C* tw, double2 scale, const double* d_norm, ObsTabs ob,
+                                   double* partials, C* mid) {
+    k_r4<C, KIN, false, 1><<<grid, r4::NT, sm, st>>>(src, nullptr, pv, tw, scale, d_norm, ob, nullptr, mid);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (!cluster) {
+        k_r4<C, KIN, false, 2><<<grid, r4::NT, sm, st>>>(nullptr, dst, pv, tw, scale, d_norm, ob, partials, mid);
+        return cudaGetLastError();
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(r4::NT);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = r4::Il<C>::v;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_r4<C, KIN, true, 2>, (const C*)nullptr, dst, pv, tw, scale, d_norm, ob, partials,
+                              mid);
 }
 
 template <class C>
@@ -1888,6 +1934,18 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
                                                (const C*)p->tw64, make_double2(p->pot_scale, 0.0), nullptr, p->ob,
                                                p->partials)));
             WIG_LAUNCHED("k_r4p");
+            return WIG_OK;
+        }
+        if (p->r4split && part < 2) {
+            C* M = reinterpret_cast<C*>(p->mid);
+            if (part == 0)
+                WIG_CUDA((launch_r4_split<C, true>(p->r4_cluster, nplanes, sm, st, P, W, pv, (const C*)p->tw64,
+                                                   make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr, M)));
+            else
+                WIG_CUDA((launch_r4_split<C, false>(p->r4_cluster, nplanes, sm, st, W, P,
+                                                    pv + (size_t)p->shape[0] * p->shape[2] * 128, (const C*)p->tw64,
+                                                    make_double2(p->pot_scale, 0.0), nullptr, p->ob, p->partials, M)));
+            WIG_LAUNCHED("k_r4 split");
             return WIG_OK;
         }
         if (part == 0) {

@@ -343,6 +343,28 @@ def test_r4p_matches_r4(dtype, monkeypatch):
     assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < 1e-13
 
 
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_r4_split_bitwise(dtype, monkeypatch):
+    """k_r4 as two launches per half-step (WIG_R4_SPLIT: forward half to a
+    scratch buffer, inverse half from it) runs the same arithmetic: the same
+    bits in the history and the state."""
+    from configs import cat_xp
+    p, c = config2(12, 64)
+    f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    monkeypatch.setenv("WIG_R4_SPLIT", "1")
+    f2 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    monkeypatch.delenv("WIG_R4_SPLIT")
+    W0 = cat_xp(f1._coords, c).astype(dtype)
+    for f in (f1, f2):
+        f.W_init_gpu.set(W0)
+        f.timeSteps = 7
+        f.fileName = None
+        f.Run()
+    for name in OBS:
+        assert np.array_equal(getattr(f1, name), getattr(f2, name)), name
+    assert np.array_equal(f1.W_init_gpu.get(), f2.W_init_gpu.get())
+
+
 def _notebook_windows(p):
     """The reference notebooks' ambiguity windows (delta N != 1)."""
     p.update(theta_x_amplitude=9.0, theta_y_amplitude=9.0, lambda_x_amplitude=9.0, lambda_y_amplitude=9.0)
