@@ -115,8 +115,9 @@ struct PlaneCfg {
     static constexpr int LD = NX + 1;                 // padded row stride
     static constexpr int PTS = NY * NX;
     static constexpr int PER = (PTS + NT - 1) / NT;   // points per thread
-    // two CTAs per SM (64 registers) while a thread holds at most 8 points
-    static constexpr int MINB = (NT >= 512 && PER <= 8) ? 2 : 1;
+    // two CTAs per SM while a thread holds at most 8 (512 threads) or 16
+    // (256 threads) points
+    static constexpr int MINB = ((NT >= 512 && PER <= 8) || (NT == 256 && PER <= 16)) ? 2 : 1;
 };
 
 template <class C, int NY, int NX>
@@ -291,6 +292,9 @@ __global__ void __launch_bounds__(NT, PlaneCfg<NPY, NPX, NT>::MINB) k_potential(
 template <class C, int NPY, int NPX, int G>
 struct PotCfg {
     static constexpr int NT = 256;
+    // complex64 planes of at most 48 x 48 points: two CTAs per SM (the
+    // dispatch halves G); complex128 would spill at that register budget
+    static constexpr int MINB = (sizeof(C) == 8 && NPY * NPX <= 48 * 48) ? 2 : 1;
     static constexpr int LD = NPX + 1;                              // row stride
     static constexpr int PSP = ((NPY * LD + 13) / 16) * 16 + 2;     // plane stride, = 2 (mod 16)
     static constexpr int PTS = NPY * NPX;
@@ -301,7 +305,7 @@ struct PotCfg {
 
 
 template <class C, int NPY, int NPX, int G>
-__global__ void __launch_bounds__(256, 1) k_potential_g(C* __restrict__ W, int ny, int nx, FactorSet<C> F,
+__global__ void __launch_bounds__(256, (PotCfg<C, NPY, NPX, G>::MINB)) k_potential_g(C* __restrict__ W, int ny, int nx, FactorSet<C> F,
                                                         double2 scale, ObsTabs ob, double* __restrict__ partials) {
     typedef PotCfg<C, NPY, NPX, G> P;
     constexpr int NT = P::NT;
@@ -1073,7 +1077,8 @@ static bool launch_potential_gn(wig4d_plan* p, C* W, double* partials, cudaStrea
 template <class C, int NPY, int NPX>
 static bool launch_potential_g(wig4d_plan* p, C* W, double* partials, cudaStream_t st, double2 sc) {
     if (getenv("WIG_NO_POT_G")) return false;
-    return launch_potential_gn<C, NPY, NPX, (sizeof(C) == 16 ? 4 : 8)>(p, W, partials, st, sc);
+    constexpr int G0 = sizeof(C) == 16 ? 4 : (NPY * NPX <= 48 * 48 ? 4 : 8);
+    return launch_potential_gn<C, NPY, NPX, G0>(p, W, partials, st, sc);
 }
 
 template <class C>
