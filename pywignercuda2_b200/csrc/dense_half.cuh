@@ -97,7 +97,7 @@ constexpr size_t dense_half_smem_bytes(bool two_matrices) {
 template <class C, int N, bool KIN>
 __global__ void __launch_bounds__(dense_half::NT, 1)
 k_dense_half(C* __restrict__ W, int n_f1, const C* __restrict__ Mr, const C* __restrict__ Mc, int neg_r, int neg_c,
-             FactorSet<C> F, double2 scale, const double* __restrict__ d_norm, ObsTabs ob,
+             const __grid_constant__ FactorSet<C> F, double2 scale, const double* __restrict__ d_norm, ObsTabs ob,
              double* __restrict__ partials, int nx_o) {
     using namespace dense_half;
     constexpr int LD = N + 1, PTS = N * N;

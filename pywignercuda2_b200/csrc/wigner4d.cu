@@ -54,9 +54,28 @@ __device__ __forceinline__ int sel4(int a, int i0, int i1, int i2, int i3) {
 
 // Product of the factor tables at point (i0, i1, i2, i3); lin is the point's
 // linear index in the array (used by full 4-D tables).
+// The loop over the tables stays rolled: kernels call this at every point
+// they hold, and the unrolled form (WIG_MAX_FACTORS bodies per call) made
+// them miss in the instruction cache.
 template <class C>
 __device__ __forceinline__ C factor_at(const FactorSet<C>& F, int i0, int i1, int i2, int i3,
                                        long long lin, C acc) {
+#pragma unroll 1
+    for (int t = 0; t < F.n; ++t) {
+        long long idx;
+        if (F.ia[t] < 0) idx = lin;
+        else if (F.ib[t] < 0) idx = sel4(F.ia[t], i0, i1, i2, i3);
+        else idx = (long long)sel4(F.ia[t], i0, i1, i2, i3) * F.nb[t] + sel4(F.ib[t], i0, i1, i2, i3);
+        acc = cmul(acc, __ldg(F.data[t] + idx));
+    }
+    return acc;
+}
+
+// The same product with the table loop unrolled (constant table indices):
+// faster where a kernel calls it at few sites (the potential kernels).
+template <class C>
+__device__ __forceinline__ C factor_at_unrolled(const FactorSet<C>& F, int i0, int i1, int i2, int i3,
+                                                long long lin, C acc) {
 #pragma unroll
     for (int t = 0; t < WIG_MAX_FACTORS; ++t) {
         if (t < F.n) {
@@ -130,7 +149,7 @@ static constexpr size_t plane_bytes() {
 // ---------------------------------------------------------------------------
 template <class C, int NY, int NX, int NT>
 __global__ void __launch_bounds__(NT, PlaneCfg<NY, NX, NT>::MINB) k_kinetic(C* __restrict__ W, int npy, int npx,
-                                                FactorSet<C> F, double2 scale,
+                                                const __grid_constant__ FactorSet<C> F, double2 scale,
                                                 const double* __restrict__ d_norm) {
     typedef PlaneCfg<NY, NX, NT> P;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -198,7 +217,7 @@ __global__ void __launch_bounds__(NT, PlaneCfg<NY, NX, NT>::MINB) k_kinetic(C* _
 // ---------------------------------------------------------------------------
 template <class C, int NPY, int NPX, int NT>
 __global__ void __launch_bounds__(NT, PlaneCfg<NPY, NPX, NT>::MINB) k_potential(C* __restrict__ W, int ny, int nx,
-                                                  FactorSet<C> F, double2 scale, ObsTabs ob,
+                                                  const __grid_constant__ FactorSet<C> F, double2 scale, ObsTabs ob,
                                                   double* __restrict__ partials) {
     typedef PlaneCfg<NPY, NPX, NT> P;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -240,7 +259,7 @@ __global__ void __launch_bounds__(NT, PlaneCfg<NPY, NPX, NT>::MINB) k_potential(
         const int e = threadIdx.x + i * NT;
         if (P::PTS % NT == 0 || e < P::PTS) {
             const int py = e / NPX, px = e % NPX;
-            C f = factor_at(F, py, iy, px, ix, lin0 + py * pys + px * pxs, cc);
+            C f = factor_at_unrolled(F, py, iy, px, ix, lin0 + py * pys + px * pxs, cc);
             s[py * P::LD + px] = cmul(s[py * P::LD + px], f);
         }
     }
@@ -305,7 +324,7 @@ struct PotCfg {
 
 
 template <class C, int NPY, int NPX, int G>
-__global__ void __launch_bounds__(256, (PotCfg<C, NPY, NPX, G>::MINB)) k_potential_g(C* __restrict__ W, int ny, int nx, FactorSet<C> F,
+__global__ void __launch_bounds__(256, (PotCfg<C, NPY, NPX, G>::MINB)) k_potential_g(C* __restrict__ W, int ny, int nx, const __grid_constant__ FactorSet<C> F,
                                                         double2 scale, ObsTabs ob, double* __restrict__ partials) {
     typedef PotCfg<C, NPY, NPX, G> P;
     constexpr int NT = P::NT;
@@ -339,7 +358,7 @@ __global__ void __launch_bounds__(256, (PotCfg<C, NPY, NPX, G>::MINB)) k_potenti
         const int ky = (py + NPY / 2) % NPY, kx = (px + NPX / 2) % NPX, ix = x0 + g;
         const long long lin = ky * pys + (long long)iy * NPX * nx + (long long)kx * nx + ix;
         C* q = s + g * P::PSP + py * P::LD + px;
-        *q = cmul(*q, factor_at(F, ky, iy, kx, ix, lin, cc));
+        *q = cmul(*q, factor_at_unrolled(F, ky, iy, kx, ix, lin, cc));
     }
     __syncthreads();
     for (int g = 0; g < G; ++g) {
@@ -401,7 +420,7 @@ __global__ void __launch_bounds__(256, (PotCfg<C, NPY, NPX, G>::MINB)) k_potenti
 // ---------------------------------------------------------------------------
 template <class C>
 __global__ void __launch_bounds__(lanes64::NT, 2) k_kin64(const C* __restrict__ W, C* __restrict__ T,
-                                                          int npy, int npx, FactorSet<C> F, double2 scale,
+                                                          int npy, int npx, const __grid_constant__ FactorSet<C> F, double2 scale,
                                                           const double* __restrict__ d_norm) {
     using namespace lanes64;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -456,7 +475,7 @@ __global__ void __launch_bounds__(lanes64::NT, 2) k_kin64(const C* __restrict__ 
 
 template <class C>
 __global__ void __launch_bounds__(lanes64::NT, 2) k_pot64(const C* __restrict__ T, C* __restrict__ W,
-                                                          int ny, int nx, FactorSet<C> F, double2 scale,
+                                                          int ny, int nx, const __grid_constant__ FactorSet<C> F, double2 scale,
                                                           ObsTabs ob, double* __restrict__ partials) {
     using namespace lanes64;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -545,7 +564,7 @@ __global__ void __launch_bounds__(lanes64::NT, 2) k_pot64(const C* __restrict__ 
 // separable part of the factor.  Tables over both in-plane axes or full
 // tables stay per point (the kernels test `pp`).
 template <class C>
-__global__ void k_plane_vectors(FactorSet<C> F, int ay, int ax, int f0, int f1, int n_f1, int nplanes,
+__global__ void k_plane_vectors(const __grid_constant__ FactorSet<C> F, int ay, int ax, int f0, int f1, int n_f1, int nplanes,
                                 C* __restrict__ PV) {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)nplanes * 128) return;
@@ -926,7 +945,7 @@ __global__ void __launch_bounds__(1024) k_finalize(const double* __restrict__ pa
 
 // Factor applied alone (unfused path): elementwise over the whole array.
 template <class C>
-__global__ void k_apply_factor(C* W, int n0, int n1, int n2, int n3, FactorSet<C> F, double2 scale) {
+__global__ void k_apply_factor(C* W, int n0, int n1, int n2, int n3, const __grid_constant__ FactorSet<C> F, double2 scale) {
     const long long tot = (long long)n0 * n1 * n2 * n3;
     const C cc = to_c<C>(scale);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
@@ -1031,6 +1050,8 @@ template <class C> static FactorSet<C>& pot_set(wig4d_plan* p);
 template <> FactorSet<double2>& pot_set<double2>(wig4d_plan* p) { return p->pot_d; }
 template <> FactorSet<float2>& pot_set<float2>(wig4d_plan* p) { return p->pot_f; }
 
+#include "k48.cuh"
+
 // Dispatch a fused kernel over the supported plane sizes.
 #define WIG_PLANE_CASES(X) X(16, 16) X(32, 32) X(48, 48) X(64, 64) X(128, 128) X(64, 128) X(128, 64)
 
@@ -1040,6 +1061,13 @@ static int launch_kinetic(wig4d_plan* p, C* W, const double* d_norm, cudaStream_
     const int npy = p->shape[0], npx = p->shape[2];
     const unsigned grid = (unsigned)(npy * npx);
     const double2 sc = make_double2(p->kin_scale, 0.0);
+    if (NY == 48 && NX == 48 && !getenv("WIG_NO_K48")) {   // 48 x 48 planes in registers
+        const size_t sm = k48::smem_bytes<C>();
+        WIG_CUDA(cudaFuncSetAttribute(k_kin48<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_kin48<C><<<grid, k48::NT, sm, st>>>(W, npy, npx, kin_set<C>(p), sc, d_norm);
+        WIG_LAUNCHED("k_kin48");
+        return WIG_OK;
+    }
 #define KCASE(a, b)                                                                      \
     if (NY == a && NX == b) {                                                            \
         constexpr int NT = FusedNT<a, b>::v;                                             \

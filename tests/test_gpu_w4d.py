@@ -276,6 +276,31 @@ def test_run_48_radix3_parity(dtype, tol):
     assert rel_err(f.W_init_gpu.get(), Wo) < (1e-10 if tol < 1e-6 else 1e-3)
 
 
+@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-13), (np.complex64, 2e-5)])
+def test_k48_matches_generic(dtype, tol, monkeypatch):
+    """The register-blocked 48 x 48 kinetic half-step (k_kin48: 3 x 3 DFTs,
+    then 16 x 16 sub-plane DFTs) against the generic k_kinetic (WIG_NO_K48)."""
+    p, c = config1(6, 48)
+    f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    monkeypatch.setenv("WIG_NO_K48", "1")
+    f2 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+    W0 = (np.random.default_rng(3).standard_normal(f1.shape) * 1e-3).astype(dtype)
+    out = []
+    for f, env in ((f1, False), (f2, True)):
+        if env:
+            monkeypatch.setenv("WIG_NO_K48", "1")
+        else:
+            monkeypatch.delenv("WIG_NO_K48", raising=False)
+        f.W_init_gpu.set(W0)
+        f.timeSteps = 4
+        f.fileName = None
+        f.Run()
+        out.append((f.norm, f.energy, f.W_init_gpu.get()))
+    monkeypatch.delenv("WIG_NO_K48", raising=False)
+    for a, b in zip(out[0], out[1]):
+        assert rel_err(a, b) < tol
+
+
 @pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-12), (np.complex64, 1e-4)])
 def test_r4_matches_pair_kernels(dtype, tol, monkeypatch):
     """The default 64^4 kernels (k_r4 with cluster stores) against
