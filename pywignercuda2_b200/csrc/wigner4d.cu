@@ -1115,6 +1115,17 @@ static int launch_potential(wig4d_plan* p, C* W, double* partials, cudaStream_t 
     const int ny = p->shape[1], nx = p->shape[3];
     const unsigned grid = (unsigned)(ny * nx);
     const double2 sc = make_double2(p->pot_scale, 0.0);
+    // k_pot48 (48 x 48 planes in registers) is selectable with WIG_POT48; it
+    // runs one CTA of 512 / 1024 threads per SM and measured slower than
+    // k_potential_g (416 against 316 us at 48^4 complex128)
+    if (NPY == 48 && NPX == 48 && nx % pot48_g<C>() == 0 && getenv("WIG_POT48") && !getenv("WIG_NO_K48")) {
+        const size_t sm = pot48_smem_bytes<C>();
+        WIG_CUDA(cudaFuncSetAttribute(k_pot48<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_pot48<C><<<(unsigned)(ny * (nx / pot48_g<C>())), k48::NT * pot48_g<C>(), sm, st>>>(
+            W, ny, nx, pot_set<C>(p), sc, p->ob, partials);
+        WIG_LAUNCHED("k_pot48");
+        return WIG_OK;
+    }
 #define PCASE(a, b)                                                                      \
     if (NPY == a && NPX == b) {                                                          \
         if (launch_potential_g<C, a, b>(p, W, partials, st, sc)) return WIG_OK;           \

@@ -276,10 +276,14 @@ def test_run_48_radix3_parity(dtype, tol):
     assert rel_err(f.W_init_gpu.get(), Wo) < (1e-10 if tol < 1e-6 else 1e-3)
 
 
+@pytest.mark.parametrize("pot48", [False, True])
 @pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-13), (np.complex64, 2e-5)])
-def test_k48_matches_generic(dtype, tol, monkeypatch):
+def test_k48_matches_generic(dtype, tol, pot48, monkeypatch):
     """The register-blocked 48 x 48 kinetic half-step (k_kin48: 3 x 3 DFTs,
-    then 16 x 16 sub-plane DFTs) against the generic k_kinetic (WIG_NO_K48)."""
+    then 16 x 16 sub-plane DFTs), and with WIG_POT48 the potential one
+    (k_pot48), against the generic k_kinetic / k_potential_g (WIG_NO_K48)."""
+    if pot48:
+        monkeypatch.setenv("WIG_POT48", "1")
     p, c = config1(6, 48)
     f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
     monkeypatch.setenv("WIG_NO_K48", "1")
