@@ -36,6 +36,7 @@ extern "C" {
 #define WIG_ERR_NONFINITE      5   /* a reduction saw NaN or Inf              */
 #define WIG_ERR_ALIAS          6   /* two component pointers alias            */
 #define WIG_ERR_TOO_LARGE      7   /* size above a fixed limit of the call    */
+#define WIG_ERR_TIMEOUT        8   /* a bounded device wait gave up           */
 
 #define WIG_C128 0
 #define WIG_C64  1
@@ -66,10 +67,12 @@ int wig_faft(void* data, const int shape[4], int dtype, int axis,
  * (GPU_Wigner4D.py:34-35, 43-44, 51-55):
  *   int FAFTxx_4D_Z2Z(void* dev_ptr, double d, double delta,
  *                     int segment, int axes, double NF);
- * FAFT64_4D_Z2Z and IFAFT64_4D_Z2Z act on a 64^4 complex128 array;
- * FAFT128_4D_Z2Z on a (64, 64, 64, 64) array as the reference's 64x64 frames
- * use it; FAFT256_4D_Z2Z on the (64, 64, 128, 128) array of its 64x128
- * frames.  IFAFT64_4D_Z2Z is FAFT64_4D_Z2Z with delta negated (the reference
+ * FAFT64_4D_Z2Z and IFAFT64_4D_Z2Z act on a 64^4 complex128 array (the
+ * reference's 64x64 frames); FAFT128_4D_Z2Z and FAFT256_4D_Z2Z on the
+ * (64, 64, 128, 128) array of its 64x128 frames, where the reference binds
+ * them as cuda_faft64 and cuda_faft128 and calls them only from the
+ * FAFT_64_128 / Fourier_*_64_128_GPU wrappers (GPU_Wigner4D.py:372-405).
+ * The transform length is the array's extent along `axes`.  IFAFT64_4D_Z2Z is FAFT64_4D_Z2Z with delta negated (the reference
  * binds but never calls it).  segment must be 0 and NF 1, the only values
  * the reference passes.  They run on the legacy default stream.
  */
@@ -128,6 +131,18 @@ typedef struct {
     const double* energy_x;    /* V(x, y)     on [N_y][N_x]                       */
     double dv_norm;            /* dV of Norm_GPU (host precision)                 */
     double dv_obs;             /* dV of the ReductionKernels (device constants)   */
+    /* Transform engine of the Run() entry points (no counterpart in the
+       reference, whose transforms are the FAFT calls of GPU_Wigner4D.py:
+       409-427): 0 the CUDA-core kernels (radix for |delta| N = 1, dense
+       otherwise); 1 k_tc64, every 64-point transform of a half-step as a
+       dense complex GEMM on the tensor cores (tcgen05.mma kind::f16,
+       operands split into fp16 hi + lo, three products, FP32 accumulation
+       in tensor memory; the factor as float-float products of FP64
+       vectors; FP64 sums above the row level), for any delta.  1 needs
+       WIG_C64 on a 64^4 grid, factor tables that do not span both in-plane
+       axes of a half-step, positive deltas and the same |delta| on the two
+       in-plane axes of each half-step (else WIG_ERR_UNSUPPORTED).        */
+    int transform;
 } wig4d_desc;
 
 /* Number of float64 values wig4d_reduce and one wig4d_run iteration write. */
@@ -233,8 +248,10 @@ int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
    Run() kernels (1 or 0 each); info[3] which 64^4 Run() kernels: 0 none,
    1 k_half64 (plane pairs), 2 k_quad64 (complex64 quads), 3 k_r4 (16 points
    per thread, the default), 4 k_r4t (complex128 k_r4 with TMA plane loads),
-   5 k_r4p (persistent k_r4 with the next plane prefetched). */
+   5 k_r4p (persistent k_r4 with the next plane prefetched), 6 k_tc64
+   (tensor-core DFTs, wig4d_desc.transform = 1). */
 int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
+
 
 /* Bytes of device memory the plan holds (tables, partial sums). */
 long long wig4d_plan_device_bytes(const wig4d_plan* plan);

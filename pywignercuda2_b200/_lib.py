@@ -16,7 +16,8 @@ C128, C64 = 0, 1
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "unsupported shape or parameter", 3: "CUDA error",
           4: "device allocation failed", 5: "non-finite value in a reduction",
-          6: "component pointers alias", 7: "size above the limit of this call"}
+          6: "component pointers alias", 7: "size above the limit of this call",
+          8: "a bounded device wait gave up"}
 
 
 class WignerError(RuntimeError):
@@ -44,7 +45,8 @@ class Desc4D(ctypes.Structure):
                 ("coord", ctypes.POINTER(ctypes.c_double) * 4),
                 ("energy_p", ctypes.POINTER(ctypes.c_double)),
                 ("energy_x", ctypes.POINTER(ctypes.c_double)),
-                ("dv_norm", ctypes.c_double), ("dv_obs", ctypes.c_double)]
+                ("dv_norm", ctypes.c_double), ("dv_obs", ctypes.c_double),
+                ("transform", ctypes.c_int)]
 
 
 class DescDirac(ctypes.Structure):

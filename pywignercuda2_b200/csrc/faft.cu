@@ -51,6 +51,7 @@ extern "C" const char* wig_status_string(int s) {
         case WIG_ERR_NONFINITE: return "non-finite value in a reduction";
         case WIG_ERR_ALIAS: return "component pointers alias";
         case WIG_ERR_TOO_LARGE: return "size above the limit of this call";
+        case WIG_ERR_TIMEOUT: return "a bounded device wait gave up";
         default: return "unknown status";
     }
 }
@@ -279,7 +280,7 @@ extern "C" int IFAFT64_4D_Z2Z(void* p, double d, double delta, int segment, int 
     return faft_shim(p, shape, d, -delta, segment, axes, NF);
 }
 extern "C" int FAFT128_4D_Z2Z(void* p, double d, double delta, int segment, int axes, double NF) {
-    static const int shape[4] = {64, 64, 64, 64};
+    static const int shape[4] = {64, 64, 128, 128};
     return faft_shim(p, shape, d, delta, segment, axes, NF);
 }
 extern "C" int FAFT256_4D_Z2Z(void* p, double d, double delta, int segment, int axes, double NF) {

@@ -560,17 +560,18 @@ __global__ void __launch_bounds__(lanes64::NT, 2) k_pot64(const C* __restrict__ 
 
 // Per-plane factor vectors, built once at plan creation: for plane (f0, f1)
 // the row-frequency vector PV[plane][0][k] and the column-frequency vector
-// PV[plane][1][k] (k already shifted by N/2), whose outer product is the
+// PV[plane][1][k] (k shifted by `shift`: N/2 for the radix kernels, which
+// leave out the centring signs; 0 for k_tc64's centred matrices), whose outer product is the
 // separable part of the factor.  Tables over both in-plane axes or full
 // tables stay per point (the kernels test `pp`).
 template <class C>
 __global__ void k_plane_vectors(const __grid_constant__ FactorSet<C> F, int ay, int ax, int f0, int f1, int n_f1, int nplanes,
-                                C* __restrict__ PV) {
+                                C* __restrict__ PV, int shift) {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)nplanes * 128) return;
     const int plane = (int)(t >> 7), j = (int)(t & 127);
     const bool along_y = j < 64;
-    const int k = j & 63, kk = (k + 32) & 63;
+    const int k = j & 63, kk = (k + shift) & 63;
     const int i_f0 = plane / n_f1, i_f1 = plane % n_f1;
     const int axis = along_y ? ay : ax;
     double2 acc = make_double2(1.0, 0.0);
@@ -795,6 +796,7 @@ __global__ void __launch_bounds__(32 * NSUM) k_finalize_sums(const double* __res
 #include "quad64.cuh"
 #include "dense_half.cuh"
 #include "r4.cuh"
+#include "tc64.cuh"
 
 // First stage of the Run() reduction for one partial row per column (y, x):
 // CTA b folds the columns b*per .. b*per + per - 1, weighted by x, y and V of
@@ -1027,6 +1029,9 @@ struct wig4d_plan {
     int r4p_grid;                  // its CTAs: SMs x resident CTAs, a multiple of the cluster size
     void* tw64;                    // k_r4 twiddle table (64 complex of the plan's dtype)
     double* fold;                  // k_fold_columns output: FOLD_BLOCKS rows of NSUM
+    bool tc;                       // complex64 64^4 Run(): k_tc64 (tensor-core DFTs) on the LK / LP layouts
+    void* tc_bimg[2];              // k_tc64's embedded FAFT matrices of the two half-steps (shared-memory images)
+    void* tc_pv;                   // k_tc64's FP64 per-plane factor vectors (unshifted frequencies)
     CUtensorMap map_t_load;        // LA view of the ping-pong buffer (kinetic source)
     CUtensorMap map_w_load;        // LB view of the caller's state (potential source)
     const void* map_w_ptr;                 // state the W maps describe
@@ -1038,6 +1043,34 @@ struct wig4d_plan {
 };
 
 static bool pow2_16_128(int n) { return wig_radix_size(n); }
+
+// k_tc64's B operand: the centred 64-point FAFT matrix
+//   M[k][n] = exp(-2 pi i delta (n - 32)(k - 32))
+// embedded as the real 128 x 128 matrix B[(ri', k)][(ri, n)] (Re/Im of the
+// output, Re/Im of the input), times 2^B_EXP, split into fp16 hi + lo, in
+// the K-major no-swizzle layout of the kernel's shared memory: element
+// (row, col) at byte (col/8)*2048 + (row/8)*128 + (row%8)*16 + (col%8)*2.
+// The phase is reduced to [0, 1) turns in FP64 before the sine and cosine.
+static int build_tc_bimg(double delta, void** out) {
+    std::vector<__half> img(2 * 128 * 128);
+    for (int row = 0; row < 128; ++row)
+        for (int col = 0; col < 128; ++col) {
+            const int rio = row >> 6, k = row & 63, ri = col >> 6, n = col & 63;
+            double turns = delta * (double)((n - 32) * (k - 32));
+            turns -= floor(turns);
+            const double ang = 2.0 * M_PI * turns;
+            const double c = cos(ang), s = sin(ang);   // M = c - i s
+            const double b = ldexp((rio == ri) ? c : (ri == 1 ? s : -s), tc64::B_EXP);
+            const __half hi = __float2half_rn((float)b);
+            const __half lo = __float2half_rn((float)(b - (double)__half2float(hi)));
+            const int off = ((col >> 3) * 2048 + (row >> 3) * 128 + (row & 7) * 16 + (col & 7) * 2) / 2;
+            img[off] = hi;
+            img[128 * 128 + off] = lo;
+        }
+    if (cudaMalloc(out, img.size() * sizeof(__half)) != cudaSuccess) return WIG_ERR_ALLOC;
+    WIG_CUDA(cudaMemcpy(*out, img.data(), img.size() * sizeof(__half), cudaMemcpyHostToDevice));
+    return WIG_OK;
+}
 
 // Threads per CTA of the fused kernels: one radix-8 butterfly per thread and
 // pass for a 64 x 64 plane; smaller planes use fewer threads.
@@ -1245,6 +1278,9 @@ static void free_plan(wig4d_plan* p) {
     cudaFree(p->pv);
     cudaFree(p->tw64);
     cudaFree(p->fold);
+    cudaFree(p->tc_bimg[0]);
+    cudaFree(p->tc_bimg[1]);
+    cudaFree(p->tc_pv);
     delete p;
 }
 
@@ -1452,9 +1488,9 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             cudaFuncSetAttribute(k_half64<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
             cudaFuncSetAttribute(k_half64<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
             double2* pv = (double2*)p->pv;
-            k_plane_vectors<double2><<<(npl_k * 128 + 255) / 256, 256>>>(p->kin_d, 1, 3, 0, 2, p->shape[2], npl_k, pv);
+            k_plane_vectors<double2><<<(npl_k * 128 + 255) / 256, 256>>>(p->kin_d, 1, 3, 0, 2, p->shape[2], npl_k, pv, 32);
             k_plane_vectors<double2><<<(npl_p * 128 + 255) / 256, 256>>>(p->pot_d, 0, 2, 1, 3, p->shape[3], npl_p,
-                                                                        pv + (size_t)npl_k * 128);
+                                                                        pv + (size_t)npl_k * 128, 32);
         } else {
             // complex64: k_quad64 takes FP64 plane vectors, built from FP64
             // copies of the tables (the plan keeps only the float32 ones)
@@ -1489,9 +1525,9 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             }
             double2* pv = (double2*)p->pv;
             if (ok) {
-                k_plane_vectors<double2><<<(npl_k * 128 + 255) / 256, 256>>>(k64, 1, 3, 0, 2, p->shape[2], npl_k, pv);
+                k_plane_vectors<double2><<<(npl_k * 128 + 255) / 256, 256>>>(k64, 1, 3, 0, 2, p->shape[2], npl_k, pv, 32);
                 k_plane_vectors<double2><<<(npl_p * 128 + 255) / 256, 256>>>(p64, 0, 2, 1, 3, p->shape[3], npl_p,
-                                                                            pv + (size_t)npl_k * 128);
+                                                                            pv + (size_t)npl_k * 128, 32);
                 ok = cudaDeviceSynchronize() == cudaSuccess;
             }
             cudaFree(t64);
@@ -1569,6 +1605,61 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             }
         }
     }
+    // tensor-core transforms (k_tc64): complex64 64^4, separable factors,
+    // positive deltas, the same |delta| on both in-plane axes of each half-step
+    if (desc->transform == 1) {
+        const bool ok64 = desc->dtype == WIG_C64 && p->shape[0] == 64 && p->shape[1] == 64 && p->shape[2] == 64 &&
+                          p->shape[3] == 64;
+        bool ok = ok64 && separable(desc->kin, desc->n_kin, 1, 3) && separable(desc->pot, desc->n_pot, 0, 2);
+        for (int a = 0; a < 4; ++a) ok = ok && p->delta[a] > 0;
+        ok = ok && fabs(p->delta[1] - p->delta[3]) <= 1e-12 * p->delta[1] &&
+             fabs(p->delta[0] - p->delta[2]) <= 1e-12 * p->delta[0];
+        if (!ok) { free_plan(p); return WIG_ERR_UNSUPPORTED; }
+        int s;
+        if ((s = build_tc_bimg(p->delta[1], &p->tc_bimg[0])) || (s = build_tc_bimg(p->delta[0], &p->tc_bimg[1]))) {
+            free_plan(p); return s;
+        }
+        const int npl_k = 64 * 64, npl_p = 64 * 64;
+        if (!p->pingpong && cudaMalloc(&p->pingpong, (size_t)p->npts * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+        if (!p->fold && cudaMalloc(&p->fold, FOLD_BLOCKS * NSUM * sizeof(double)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+        if (cudaMalloc(&p->tc_pv, (size_t)(npl_k + npl_p) * 128 * sizeof(double2)) != cudaSuccess) {
+            free_plan(p); return WIG_ERR_ALLOC;
+        }
+        // FP64 plane vectors from FP64 copies of the host tables (the plan
+        // itself keeps the float32 tables of a complex64 state)
+        long long n64 = 0;
+        for (int i = 0; i < desc->n_kin; ++i) n64 += tab_elems(desc->kin[i]);
+        for (int i = 0; i < desc->n_pot; ++i) n64 += tab_elems(desc->pot[i]);
+        double2* t64 = nullptr;
+        if (n64 > 0 && cudaMalloc(&t64, (size_t)n64 * sizeof(double2)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+        FactorSet<double2> k64 = p->kin_d, p64 = p->pot_d;
+        long long o64 = 0;
+        bool up = true;
+        for (int i = 0; i < desc->n_kin; ++i) {
+            const long long n = tab_elems(desc->kin[i]);
+            up = up && cudaMemcpy(t64 + o64, desc->kin[i].host_data, n * 16, cudaMemcpyHostToDevice) == cudaSuccess;
+            k64.data[i] = t64 + o64; o64 += n;
+        }
+        for (int i = 0; i < desc->n_pot; ++i) {
+            const long long n = tab_elems(desc->pot[i]);
+            up = up && cudaMemcpy(t64 + o64, desc->pot[i].host_data, n * 16, cudaMemcpyHostToDevice) == cudaSuccess;
+            p64.data[i] = t64 + o64; o64 += n;
+        }
+        double2* pv = (double2*)p->tc_pv;
+        if (up) {
+            k_plane_vectors<double2><<<(npl_k * 128 + 255) / 256, 256>>>(k64, 1, 3, 0, 2, 64, npl_k, pv, 0);
+            k_plane_vectors<double2><<<(npl_p * 128 + 255) / 256, 256>>>(p64, 0, 2, 1, 3, 64, npl_p,
+                                                                        pv + (size_t)npl_k * 128, 0);
+            up = cudaDeviceSynchronize() == cudaSuccess;
+        }
+        cudaFree(t64);
+        if (!up) { wig_set_cuda_error(cudaGetLastError(), "tc plane vectors"); free_plan(p); return WIG_ERR_CUDA; }
+        if (cudaFuncSetAttribute(k_tc64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc64::SMEM) != cudaSuccess ||
+            cudaFuncSetAttribute(k_tc64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc64::SMEM) != cudaSuccess) {
+            wig_set_cuda_error(cudaGetLastError(), "k_tc64 attributes"); free_plan(p); return WIG_ERR_CUDA;
+        }
+        p->tc = true;
+    }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { wig_set_cuda_error(e, "wig4d_plan_create"); free_plan(p); return WIG_ERR_CUDA; }
     *out = p;
@@ -1585,7 +1676,7 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     if (!p || !info) return WIG_ERR_INVALID_ARG;
     info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64;
-    info[3] = !p->fast64 ? 0 : (p->r4p ? 5 : (p->r4t ? 4 : (p->r4 ? 3 : (p->quad64 ? 2 : 1))));
+    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4p ? 5 : (p->r4t ? 4 : (p->r4 ? 3 : (p->quad64 ? 2 : 1)))));
     return WIG_OK;
 }
 
@@ -1939,6 +2030,29 @@ static cudaError_t launch_r4_split(bool cluster, unsigned grid, size_t sm, cudaS
 
 template <class C>
 static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t st, int part) {
+    if constexpr (std::is_same<C, float2>::value) {
+        if (p->tc) {
+            // W holds LP, the ping-pong buffer LK (converted around the loop)
+            float2* P = reinterpret_cast<float2*>(p->pingpong);
+            const double2* pv = reinterpret_cast<const double2*>(p->tc_pv);
+            const unsigned grid = (unsigned)(wig_num_sms() < 1024 ? wig_num_sms() : 1024);
+            if (part == 0) {
+                k_tc64<true><<<grid, tc64::NT, tc64::SMEM, st>>>(P, W, pv, (const uint4*)p->tc_bimg[0],
+                                                                 make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob,
+                                                                 nullptr, p->flag);
+                WIG_LAUNCHED("k_tc64<kin>");
+            } else if (part == 1) {
+                k_tc64<false><<<grid, tc64::NT, tc64::SMEM, st>>>(W, P, pv + (size_t)p->shape[0] * p->shape[2] * 128,
+                                                                  (const uint4*)p->tc_bimg[1],
+                                                                  make_double2(p->pot_scale, 0.0), nullptr, p->ob,
+                                                                  p->partials, p->flag);
+                WIG_LAUNCHED("k_tc64<pot>");
+            } else {
+                return fold_and_finalize(p, hist, rows, st);
+            }
+            return WIG_OK;
+        }
+    }
     if constexpr (std::is_same<C, double2>::value) {
         if (p->r4t) {
             int s;
@@ -2067,6 +2181,11 @@ static int iteration(wig4d_plan* p, C* W, double* hist, int rows, cudaStream_t s
 // Before the first iteration: the complex64 64^4 loop works on the LA / LB
 // layouts (the state moves to the ping-pong buffer as LA).
 static int enter_loop_layout(wig4d_plan* p, void* W, cudaStream_t st) {
+    if (p->tc) {
+        k_to_tc_layout<<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)W, (float2*)p->pingpong, p->npts);
+        WIG_LAUNCHED("k_to_tc_layout");
+        return WIG_OK;
+    }
     if (p->r4) {
         if (p->dtype == WIG_C128)
             k_to_r4_layout<double2><<<wig_num_sms() * 8, 256, 0, st>>>((const double2*)W, (double2*)p->pingpong, p->npts);
@@ -2084,6 +2203,12 @@ static int enter_loop_layout(wig4d_plan* p, void* W, cudaStream_t st) {
 // After the last iteration: the state back in the reference layout, divided
 // by its norm (the final renormalisation, GPU_Wigner4D.py:516-517).
 static int leave_loop_layout(wig4d_plan* p, void* W, cudaStream_t st, bool divide = true) {
+    if (p->tc) {
+        k_from_tc_layout<<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)p->pingpong, (float2*)W, p->npts,
+                                                            divide ? p->cur_norm : nullptr);
+        WIG_LAUNCHED("k_from_tc_layout");
+        return WIG_OK;
+    }
     if (p->r4) {
         const double* nrm = divide ? p->cur_norm : nullptr;
         if (p->dtype == WIG_C128)

@@ -18,6 +18,9 @@ Extra attributes a frame may set (defaults reproduce the reference):
 * ``complex_dtype``: ``numpy.complex128`` (the drop-in) or
   ``numpy.complex64`` (the precision form: complex64 state, phase factors
   built in float64 and rounded once, float64 reductions).
+* ``tensor_cores``: True (complex64 64^4 grids, any delta) runs Run()'s
+  64-point transforms as dense FAFT GEMMs on the tensor cores (fp16 hi + lo
+  operands, FP32 accumulation; k_tc64) instead of the CUDA-core kernels.
 * ``round_constants``: True reproduces the reference's '%f' formatting of the
   device constants (GPU_Wigner4D.py:128-150); False uses full precision.
 * ``snapshotEvery``: K > 0 makes Run() keep the normalised state every K
@@ -49,6 +52,7 @@ class GPU_Wigner4D:
 
     complex_dtype = np.complex128
     round_constants = True
+    tensor_cores = False
 
     def __init__(self):
         require_cuda()
@@ -169,6 +173,7 @@ class GPU_Wigner4D:
         d.dv_norm = self.dx * self.dp_x * self.dy * self.dp_y
         d.dv_obs = self._c("dx") * self._c("dy") * self._c("dp_x") * self._c("dp_y")
         plan = ctypes.c_void_p()
+        d.transform = 1 if self.tensor_cores else 0
         _lib.call("wig4d_plan_create", ctypes.byref(d), ctypes.byref(plan))
         self._plan = plan
         self._desc = d
@@ -308,7 +313,7 @@ class GPU_Wigner4D:
         """Kernels the plan runs: fused_kinetic, fused_potential, fast64, run64_kernel."""
         info = (ctypes.c_int * 4)()
         _lib.call("wig4d_plan_info", self._plan, info)
-        run64 = {0: None, 1: "half64", 2: "quad64", 3: "r4", 4: "r4t", 5: "r4p"}[info[3]]
+        run64 = {0: None, 1: "half64", 2: "quad64", 3: "r4", 4: "r4t", 5: "r4p", 6: "tc"}[info[3]]
         return {"fused_kinetic": bool(info[0]), "fused_potential": bool(info[1]), "fast64": bool(info[2]),
                 "run64_kernel": run64}
 
