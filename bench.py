@@ -95,14 +95,71 @@ def _traffic():
     return out
 
 
-def _frame(dtype):
-    from configs import cat_xp, config2
+def _frame(dtype, **kw):
+    """The 64^4 workload: config 2's coefficients, the cat state built by the
+    product initialiser (psi-based W in (x, theta), then theta -> p)."""
+    from configs import config2
     from frames import make_frame
     from pywignercuda2_b200 import GPU_Wigner4D
     params, c = config2(seed=0, n=64)
-    f = make_frame(GPU_Wigner4D, params, complex_dtype=dtype)
-    W0 = cat_xp(f._coords, c).astype(dtype)
+    f = make_frame(GPU_Wigner4D, params, complex_dtype=dtype, **kw)
+    f.CatState_GPU(f.W_init_gpu, c[0], c[1], c[2], c[3], 1.5, 0.0)
+    W0 = f.W_init_gpu.get()
     return f, W0
+
+
+def _hist_err(h, ref):
+    """Relative errors of a Run() history against a reference history."""
+    def rel(a, b):
+        return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+    return {"norm_rel_max": rel(h[:, 0], ref[:, 0]), "energy_rel_max": rel(h[:, 10], ref[:, 10]),
+            "energy_rel_last": float(abs(h[-1, 10] - ref[-1, 10]) / abs(ref[-1, 10])),
+            "x_rel_max": rel(h[:, 2], ref[:, 2]), "p_x_rel_max": rel(h[:, 3], ref[:, 3]),
+            "x2_rel_max": rel(h[:, 4], ref[:, 4])}
+
+
+def accuracy_1000(steps=1000):
+    """The FP32 forms after `steps` Run() iterations against the complex128
+    drop-in from the same initial state (the drop-in matches the FP64 oracle
+    to 1e-12 over 20 iterations at 64^4 and 3 iterations on config 3's grid,
+    tests/test_gpu_tc.py and tests/test_gpu_w4d.py): the radix complex64
+    kernels and the tensor-core kernels at 64^4 (config 2), and the complex64
+    form on config 3's 64 x 128 x 64 x 128 grid."""
+    import torch
+    from configs import w4d_params
+    from frames import make_frame
+    from pywignercuda2_b200 import GPU_Wigner4D, _lib
+    out = {"steps": steps, "reference": "complex128 drop-in on the same GPU (oracle-pinned)"}
+
+    def run(f, W0):
+        h = torch.empty((steps, _lib.WIG4D_NOBS), dtype=torch.float64, device="cuda")
+        f.W_init_gpu.set(W0.astype(f.complex_dtype))
+        f.run_device(f.W_init_gpu, steps, h)
+        return h.cpu().numpy(), f.W_init_gpu.tensor.to(torch.complex128)
+
+    f, W0 = _frame(np.complex128)
+    h128, w128 = run(f, W0)
+    del f
+    for name, kw in (("c64_radix", {}), ("c64_tensor_cores", {"tensor_cores": True})):
+        g, _ = _frame(np.complex64, **kw)
+        h, w = run(g, W0)
+        e = _hist_err(h, h128)
+        e["max_dW_rel"] = (w - w128).abs().max().item() / w128.abs().max().item()
+        out["64^4_" + name] = e
+        del g, w
+    del w128
+    p = w4d_params(64, q=0.1, kappa=0.05, D=0.01, dt=0.005, n_p=128)
+    fa = make_frame(GPU_Wigner4D, p)
+    fa.HOscillatorGound_GPU(fa.W_init_gpu, 0.4, -0.3, 0.2, -0.1, 1.0, 1.0, 1.0)
+    W3 = fa.W_init_gpu.get()
+    h3, _ = run(fa, W3)
+    del fa
+    fb = make_frame(GPU_Wigner4D, p, complex_dtype=np.complex64)
+    h3b, _ = run(fb, W3)
+    del fb
+    out["config3_64x128x64x128_c64_radix"] = _hist_err(h3b, h3)
+    torch.cuda.empty_cache()
+    return out
 
 
 def cpu_baseline_port(steps, workers, budget_s=20.0):
@@ -315,6 +372,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 48-instance line")
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--no-dirac", action="store_true", help="skip the Wigner-Dirac line")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the 1000-step accuracy block")
     ap.add_argument("--dirac-steps", type=int, default=20)
     ap.add_argument("--dirac-passes", choices=["c128", "c64"],
                     help="only time each pass of one Wigner-Dirac iteration in this dtype and exit")
@@ -370,8 +428,8 @@ def main():
     W128 = f.W_init_gpu.tensor.clone()
 
     # ---- precision form (complex64) on the same workload and step count -------
-    f32, W32 = _frame(np.complex64)
-    f32.W_init_gpu.set(W32)
+    f32, _ = _frame(np.complex64)
+    f32.W_init_gpu.set(W0.astype(np.complex64))        # the same initial state, rounded
     hist32 = torch.empty_like(hist)
     f32.run_device(f32.W_init_gpu, Wm, hist32)
     torch.cuda.synchronize()
@@ -410,8 +468,7 @@ def main():
     state_bytes = P * 16
     kin_ms, pot_ms, fin_ms = [m / K for m in f.run_device_timed(f.W_init_gpu, K, hist)]
     run64 = f.plan_info()["run64_kernel"]
-    names = {"r4t": ("k_r4t<kin>", "k_r4t<pot>"), "r4": ("k_r4<kin>", "k_r4<pot>"),
-             "half64": ("k_half64<kin>", "k_half64<pot>")}.get(
+    names = {"r4t": ("k_r4t<kin>", "k_r4t<pot>"), "r4": ("k_r4<kin>", "k_r4<pot>")}.get(
         run64, ("k_kinetic", "k_potential"))
     dom_name, dom_ms = (names[1], pot_ms) if pot_ms >= kin_ms else (names[0], kin_ms)
     peaks = _peaks()
@@ -428,7 +485,7 @@ def main():
                 "step_frac": (4 * state_bytes / (ms / K / 1e3) / 1e9) / peak}
     k32, p32, _ = [m / K for m in f32.run_device_timed(f32.W_init_gpu, K, hist32)]
     d32 = max(k32, p32)
-    kname = "k_r4" if f32.plan_info()["run64_kernel"] == "r4" else "k_quad64"
+    kname = "k_r4"
     precision["roofline"] = {"bound": "hbm", "kernel": kname + ("<pot>" if p32 >= k32 else "<kin>"),
                              "achieved": state_bytes / (d32 / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                              "frac": state_bytes / (d32 / 1e3) / 1e9 / peak,
@@ -437,6 +494,41 @@ def main():
                              "traffic": _traffic().get((kname + ("<pot>" if p32 >= k32 else "<kin>"),
                                                         "64x64x64x64_c64"))}
     del f32
+
+    # ---- tensor-core form (k_tc64: the 64-point transforms as dense GEMMs on
+    # tcgen05, split fp16, FP32 accumulation) on the same workload ---------------
+    ftc, _ = _frame(np.complex64, tensor_cores=True)
+    ftc.W_init_gpu.set(W0.astype(np.complex64))
+    histtc = torch.empty_like(hist)
+    ftc.run_device(ftc.W_init_gpu, Wm, histtc)
+    torch.cuda.synchronize()
+    e0.record(st)
+    ftc.run_device(ftc.W_init_gpu, K, histtc)
+    e1.record(st)
+    torch.cuda.synchronize()
+    mstc = e0.elapsed_time(e1)
+    htc = histtc[:K].cpu().numpy()
+    ktc, ptc, _ = [m / K for m in ftc.run_device_timed(ftc.W_init_gpu, K, histtc)]
+    dtc = max(ktc, ptc)
+    # issued tensor FLOPs per launch: 2048 plane pairs x 4 stages x 3 products
+    # x (2 x 128 x 128 x 128); the dense-DFT algorithmic count is 4 transforms
+    # x 8 N flops per point
+    tc_flops = 2048 * 4 * 3 * 2 * 128 ** 3
+    dft_flops = 4 * 8 * 64 * P
+    tpeak = peaks.get("bf16_tflops_sustained") or 1400.0
+    tensor_form = {"dtype": "c64 state, fp16 hi+lo operands, FP32 accumulation", "kernel": "k_tc64",
+                   "steps_per_s": K / (mstc / 1e3), "speedup_vs_plain": (K / (mstc / 1e3)) / (K / (ms / 1e3)),
+                   "kinetic_ms": ktc, "potential_ms": ptc,
+                   "roofline": {"bound": "tensor", "kernel": "k_tc64<pot>" if ptc >= ktc else "k_tc64<kin>",
+                                "achieved": tc_flops / (dtc / 1e3) / 1e12, "peak": tpeak, "unit": "TFLOP/s",
+                                "frac": tc_flops / (dtc / 1e3) / 1e12 / tpeak,
+                                "peak_source": "measured bf16 dense, sustained" if peaks.get("bf16_tflops_sustained")
+                                else "fallback",
+                                "issued_tensor_flops_per_launch": tc_flops,
+                                "dense_dft_flops_per_launch": dft_flops,
+                                "hbm_frac": state_bytes / (dtc / 1e3) / 1e9 / peak},
+                   "error_vs_c128": dict(_hist_err(htc, h128), steps=Wm + K)}
+    del ftc
 
     # ---- end to end through the public API with host buffers ---------------------
     host_in = torch.from_numpy(W0).pin_memory()
@@ -462,8 +554,10 @@ def main():
                        "parallelism": "replicas" if ws > 1 else "single",
                        "cache": "inputs larger than L2 (268 MB state vs 126 MB L2), no flush",
                        "factor_mode": list(f._factor_mode)},
+            "value_form": "FP64 plain drop-in (complex128, oracle-exact)",
             "grid_point_steps_per_s": value * P,
             "precision_form": precision,
+            "tensor_core_form": tensor_form,
             "gpu_launches": (4 * K + 4) if run64 in ("r4", "r4t") else (3 * K + 3),
             "finite": finite, "roofline": roofline, "clocks": clocks,
             "e2e": {"value": ws * K / (e2e_ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d / K,
@@ -472,6 +566,14 @@ def main():
                             "final state read back"}}
     if not args.no_batch:
         line["batched_form"] = bench_batched(args.batch_steps)
+    if not args.no_accuracy:
+        line["accuracy_1000_steps"] = accuracy_1000(1000)
+    line["metric_ratio"] = {
+        "tensor_core_vs_plain": tensor_form["speedup_vs_plain"],
+        "fp32_radix_vs_plain": precision["speedup_vs_plain"],
+        "batched_fp32_vs_one_at_a_time_plain": line.get("batched_form", {}).get("speedup_vs_one_at_a_time_plain"),
+        "note": "steps/s ratios at 64^4 on the same GPU and step count; errors after 1000 steps are in "
+                "accuracy_1000_steps (target <= 1e-6 in norm and energy)"}
     if not args.no_dirac:
         line["dirac_form"] = bench_dirac(args.dirac_steps)
     if rank == 0 and not args.no_cpu_baseline:

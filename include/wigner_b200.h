@@ -219,6 +219,19 @@ int wig4d_init_ho_ground(wig4d_plan* plan, void* W, double x_mu, double y_mu,
 int wig4d_init_gaussian(wig4d_plan* plan, void* W, double mu_p_y, double mu_y,
                         double mu_p_x, double mu_x, double s_p_y, double s_y,
                         double s_p_x, double s_x, void* stream);
+/*
+ * Two displaced Gaussians in superposition on the (x, theta) grid (no
+ * reference initialiser; built as WignerDiracGaussian_ParticleUp_GPU builds
+ * its spinor, GPU_WignerDirac4D.py:939-968):
+ *   W = psi(x - theta/2) conj(psi(x + theta/2)),
+ *   psi = [g(x - x_mu - a_x, y - y_mu - a_y) + g(x - x_mu + a_x, y - y_mu + a_y)]
+ *         exp(i (p_x_mu x + p_y_mu y)),  g(u, v) = exp(-(u^2 + v^2) / 2),
+ * theta_q = dtheta_q (i_q - N_q/2) along axes 0 (theta_y) and 2 (theta_x).
+ * Fourier_Theta_To_P afterwards gives the Wigner function on the (x, p) grid.
+ */
+int wig4d_init_cat_xtheta(wig4d_plan* plan, void* W, double dtheta_y, double dtheta_x,
+                          double x_mu, double y_mu, double p_x_mu, double p_y_mu,
+                          double a_x, double a_y, void* stream);
 
 /*
  * Observables of a state without any device allocation.  This entry point
@@ -232,8 +245,8 @@ int wig4d_init_gaussian(wig4d_plan* plan, void* W, double mu_p_y, double mu_y,
  * library (WIG4D_NOALLOC_MAX_COLUMNS * 12 doubles, 1.5 MiB, held by every GPU
  * that loads the library until the process exits); grids with
  * N_y * N_x > WIG4D_NOALLOC_MAX_COLUMNS return WIG_ERR_TOO_LARGE.  The first
- * call on a device looks up the array's device address, so make it before
- * any stream capture.  All calls share the array: calls whose kernels
+ * call on a device looks up the array's device address (again after the
+ * device's context was reset), so make it before any stream capture.  All calls share the array: calls whose kernels
  * overlap on the GPU race; calls ordered on one stream do not.
  */
 #define WIG4D_NOALLOC_MAX_COLUMNS 16384
@@ -245,11 +258,10 @@ int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
 
 /* Which kernels a plan runs (no counterpart in the reference): info[0] fused
    kinetic half-step, info[1] fused potential half-step, info[2] the 64^4
-   Run() kernels (1 or 0 each); info[3] which 64^4 Run() kernels: 0 none,
-   1 k_half64 (plane pairs), 2 k_quad64 (complex64 quads), 3 k_r4 (16 points
-   per thread, the default), 4 k_r4t (complex128 k_r4 with TMA plane loads),
-   5 k_r4p (persistent k_r4 with the next plane prefetched), 6 k_tc64
-   (tensor-core DFTs, wig4d_desc.transform = 1). */
+   radix Run() kernels (1 or 0 each); info[3] the 64^4 Run() kernels: 0 none,
+   3 k_r4 (16 points per thread, the default), 4 k_r4t (complex128 k_r4 with
+   TMA plane loads, WIG_FAST64_KERNEL=r4t), 6 k_tc64 (tensor-core transforms,
+   wig4d_desc.transform = 1). */
 int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
 
 
@@ -290,6 +302,11 @@ typedef struct {
                                   [3][2 sides][a_rank][N_x*N_px + N_y*N_py]        */
     const double* obs_xy;      /* [7][N_y][N_x]: A0 A1 A2 A3 D1A0 D1A1 D1A2        */
     double dv_norm, dv_obs;
+    /* Fields without a low-rank form (a_rank = 0): A1, A2, A3 at x -+ theta/2
+       on every point of the (x, theta) grid, [3][2 sides][N_py*N_y*N_px*N_x]
+       in the state's layout; NULL when the rank tables are used.  The
+       reference evaluates any expression there (GPU_WignerDirac4D.py:580-604). */
+    const double* a_full;
 } wigd_desc;
 
 /* values per observables row: norm_re, norm_im, <x>, <p_x>, <x^2>, <p_x^2>, <y>,

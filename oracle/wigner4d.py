@@ -87,6 +87,22 @@ class Wigner4DOracle:
         t = t * np.exp(-0.5 * (py - mu_p_y) ** 2 / s_p_y ** 2)
         return t.astype(np.complex128)
 
+    def cat_xtheta(self, x_mu, y_mu, p_x_mu, p_y_mu, a_x, a_y):
+        """Two displaced Gaussians in superposition on the (x, theta) grid,
+        W = psi(x - theta/2) conj(psi(x + theta/2)) -- the construction of
+        WignerDiracGaussian_ParticleUp_GPU (WD4D:939-968) applied to
+        psi = [g(q - q_mu - a) + g(q - q_mu + a)] exp(i p_mu . q),
+        g = exp(-|q|^2 / 2).  p_to_theta(W, -1) then gives (x, p)."""
+        x, tx = self._axis(3, self.dx), self._axis(2, self.dtheta_x)
+        y, ty = self._axis(1, self.dy), self._axis(0, self.dtheta_y)
+
+        def psi(u, v):
+            g = (np.exp(-0.5 * ((u - x_mu - a_x) ** 2 + (v - y_mu - a_y) ** 2))
+                 + np.exp(-0.5 * ((u - x_mu + a_x) ** 2 + (v - y_mu + a_y) ** 2)))
+            return g * np.exp(1j * (p_x_mu * u + p_y_mu * v))
+
+        return (psi(x - 0.5 * tx, y - 0.5 * ty) * np.conj(psi(x + 0.5 * tx, y + 0.5 * ty))).astype(np.complex128)
+
     # ---- reductions -----------------------------------------------------
     def norm(self, W):
         """Norm_GPU, W4D:367-369 (host-precision dV, complex)."""

@@ -62,7 +62,8 @@ class DescDirac(ctypes.Structure):
                 ("n_phase", ctypes.c_int), ("phase", Factor * WIG_MAX_FACTORS),
                 ("a_rank", ctypes.c_int), ("a_tabs", ctypes.POINTER(ctypes.c_double)),
                 ("obs_xy", ctypes.POINTER(ctypes.c_double)),
-                ("dv_norm", ctypes.c_double), ("dv_obs", ctypes.c_double)]
+                ("dv_norm", ctypes.c_double), ("dv_obs", ctypes.c_double),
+                ("a_full", ctypes.POINTER(ctypes.c_double))]
 
 
 WIGD_NOBS = 19
@@ -102,6 +103,7 @@ SIGNATURES = {
     "wig4d_run_batch": [_P, _P, _I, _I, _P, _P],
     "wig4d_init_ho_ground": [_P, _P, _D, _D, _D, _D, _D, _D, _D, _P],
     "wig4d_init_gaussian": [_P, _P, _D, _D, _D, _D, _D, _D, _D, _D, _P],
+    "wig4d_init_cat_xtheta": [_P, _P, _D, _D, _D, _D, _D, _D, _D, _D, _P],
     "wig4d_plan_device_bytes": [_P],
     "wig4d_observables_noalloc": [_P, _IP, _I, _P, _P, _P, _P, _P, _P, _D, _D, _P, _P],
     "wigd_plan_create": [ctypes.POINTER(DescDirac), ctypes.POINTER(_P)],

@@ -75,6 +75,7 @@ struct DParams {
     const double* obs_xy;                          // [7][N1][N3]
     int pow2, s3, s32, s321;                       // all sizes powers of two: shifts of axes 2, 1, 0
     int a3zero;                                    // A3 vanishes on both Bopp sides (rank tables)
+    const double* afull;                           // or full tables [3][2][points] in the state layout
 };
 
 // Point index -> (i0, i1, i2, i3) in 32-bit arithmetic (plans hold fewer
@@ -218,6 +219,8 @@ __device__ __forceinline__ M4 pot_matrix(double A1, double A2, double A3, double
 // side 1 = (x + theta/2); indices ix (axis 3), itx (axis 2), iy (axis 1), ity (axis 0).
 __device__ __forceinline__ double a_field(const DParams& P, int k, int side, int ix, int itx, int iy, int ity) {
     const long long nu = (long long)P.n3 * P.n2, nv = (long long)P.n1 * P.n0;
+    if (P.afull)
+        return P.afull[(long long)(k * 2 + side) * nu * nv + (((long long)ity * P.n1 + iy) * P.n2 + itx) * P.n3 + ix];
     const double* base = P.atab + ((long long)(k * 2 + side) * P.arank) * (nu + nv);
     double acc = 0.0;
     for (int r = 0; r < P.arank; ++r) {
@@ -690,6 +693,7 @@ struct wigd_plan {
     int* flag;
     int nblk;
     void* tw64;              // twiddles of k_dplane_r4 (64^4 grids only)
+    double* afull;           // full A1..A3 tables (fields that are not of low rank)
 };
 
 static unsigned dgrid(long long n, int threads = 256, int per_sm = 8) {
@@ -704,6 +708,7 @@ static void free_dplan(wigd_plan* p) {
     cudaFree(p->partials);
     cudaFree(p->cur_norm);
     cudaFree(p->tw64);
+    cudaFree(p->afull);
     delete p;
 }
 
@@ -716,6 +721,7 @@ extern "C" int wigd_plan_create(const wigd_desc* desc, wigd_plan** out) {
         if (!desc->coord[a] || !desc->acoord[a] || !desc->mask_xp[a] || !desc->mask_p[a]) return WIG_ERR_INVALID_ARG;
     }
     if (desc->a_rank < 0 || desc->a_rank > 16 || (desc->a_rank > 0 && !desc->a_tabs) || !desc->obs_xy ||
+        (desc->a_full && desc->a_rank != 0) ||
         desc->n_phase < 0 || desc->n_phase > WIG_MAX_FACTORS)
         return WIG_ERR_INVALID_ARG;
     wigd_plan* p = new wigd_plan();
@@ -777,6 +783,15 @@ extern "C" int wigd_plan_create(const wigd_desc* desc, wigd_plan** out) {
             for (long long e = 0; e < nv && vz; ++e) vz = f[nu + e] == 0.0;
             if (!uz && !vz) { P.a3zero = 0; break; }
         }
+    if (desc->a_full) {
+        // fields without a low-rank form: A_k at both Bopp sides on every point
+        const size_t nb = 6 * (size_t)p->npts * sizeof(double);
+        if (cudaMalloc(&p->afull, nb) != cudaSuccess) { free_dplan(p); return WIG_ERR_ALLOC; }
+        cudaMemcpy(p->afull, desc->a_full, nb, cudaMemcpyHostToDevice);
+        P.afull = p->afull;
+        P.a3zero = 1;
+        for (long long e = 4 * p->npts; e < 6 * p->npts && P.a3zero; ++e) P.a3zero = desc->a_full[e] == 0.0;
+    }
     P.obs_xy = D + off_o;
     // ---- A0 phase factor tables ----
     auto tab_elems = [&](const wig_factor& f) -> long long {

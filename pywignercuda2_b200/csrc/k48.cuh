@@ -195,97 +195,3 @@ __global__ void __launch_bounds__(k48::NT) k_kin48(C* __restrict__ W, int npy, i
         for (int b = 0; b < 3; ++b)
             g[(n2r + 16 * a) * rowstride + n2c + 16 * b] = neg ? cneg(u[3 * a + b]) : u[3 * a + b];
 }
-
-// k_pot48: the fused potential half-step on 48 x 48 (p_y, p_x) planes, the
-// contract of k_potential_g<C, 48, 48, G>: a CTA takes the G columns x0 ..
-// x0 + G - 1 at one y (G = 2 complex128, 4 complex64: 32-byte runs),
-// gathered by cp.async into one 9 * PS-element buffer per column; group g of
-// 256 threads transforms column g with k48::transform.  No centring signs:
-// the factor is read at frequencies shifted by 24.  Each group then writes
-// its column's NPART partial sums, as k_potential_g does.
-template <class C>
-constexpr int pot48_g() { return sizeof(C) == 16 ? 2 : 4; }
-template <class C>
-constexpr size_t pot48_smem_bytes() {
-    return sizeof(C) * ((size_t)pot48_g<C>() * 9 * k48::PS + 48) + sizeof(double) * NPART * 8 * pot48_g<C>();
-}
-
-template <class C>
-__global__ void __launch_bounds__(k48::NT * pot48_g<C>(), 1)
-k_pot48(C* __restrict__ W, int ny, int nx, const __grid_constant__ FactorSet<C> F, double2 scale, ObsTabs ob,
-        double* __restrict__ partials) {
-    using namespace k48;
-    constexpr int G = pot48_g<C>();
-    constexpr int NTB = NT * G;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* s = reinterpret_cast<C*>(smraw);
-    C* tw = s + G * 9 * PS;
-    double* red = reinterpret_cast<double*>(tw + 48);
-    const int grp = threadIdx.x >> 8, t = threadIdx.x & 255;
-    const int nxg = nx / G;
-    const int x0 = (blockIdx.x % nxg) * G, iy = blockIdx.x / nxg;
-    const long long pys = (long long)ny * 48 * nx;      // stride of p_y
-    C* gb = W + (long long)iy * 48 * nx + x0;           // element (p_y, p_x, g): gb[p_y*pys + p_x*nx + g]
-    for (int e = threadIdx.x; e < G * 48 * 48; e += NTB) {
-        const int g = e % G, px = (e / G) % 48, py = e / (G * 48);
-        cp_async_elem(s + g * 9 * PS + py * 49 + px, gb + py * pys + (long long)px * nx + g);
-    }
-    make_twiddles(tw, 48);
-    const C cc = to_c<C>(scale);
-    cp_async_wait_all();
-    __syncthreads();
-    C* sg = s + grp * 9 * PS;
-    const int n2r = t >> 4, n2c = t & 15;
-    C u[9];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int b = 0; b < 3; ++b) u[3 * a + b] = sg[(n2r + 16 * a) * 49 + n2c + 16 * b];
-    __syncthreads();                                   // the gathered planes have been read
-    const int ix = x0 + grp;
-    transform(u, sg, tw, t, [&](int y, int x) {
-        const int ky = (y + 24) % 48, kx = (x + 24) % 48;
-        const long long lin = ky * pys + (long long)iy * 48 * nx + (long long)kx * nx + ix;
-        return factor_at_unrolled(F, ky, iy, kx, ix, lin, cc);
-    });
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int b = 0; b < 3; ++b) gb[(n2r + 16 * a) * pys + (long long)(n2c + 16 * b) * nx + grp] = u[3 * a + b];
-    if (!partials) return;
-    double acc[NPART];
-#pragma unroll
-    for (int i = 0; i < NPART; ++i) acc[i] = 0.0;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const int py = n2r + 16 * a;
-        const double qy = __ldg(ob.cpy + py);
-#pragma unroll
-        for (int b = 0; b < 3; ++b) {
-            const int px = n2c + 16 * b;
-            const double2 w = to_d2(u[3 * a + b]);
-            const double qx = __ldg(ob.cpx + px), k = __ldg(ob.ep + py * 48 + px);
-            acc[0] += w.x; acc[1] += w.y;
-            acc[2] = fma(qx, w.x, acc[2]); acc[3] = fma(qx, w.y, acc[3]);
-            acc[4] = fma(qx * qx, w.x, acc[4]); acc[5] = fma(qx * qx, w.y, acc[5]);
-            acc[6] = fma(qy, w.x, acc[6]); acc[7] = fma(qy, w.y, acc[7]);
-            acc[8] = fma(qy * qy, w.x, acc[8]); acc[9] = fma(qy * qy, w.y, acc[9]);
-            acc[10] = fma(k, w.x, acc[10]); acc[11] = fma(k, w.y, acc[11]);
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < NPART; ++i)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc[i] += __shfl_down_sync(0xffffffffu, acc[i], o);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0)
-#pragma unroll
-        for (int i = 0; i < NPART; ++i) red[w * NPART + i] = acc[i];
-    __syncthreads();
-    if (threadIdx.x < G * NPART) {
-        const int gg = threadIdx.x / NPART, i = threadIdx.x % NPART;
-        double sum = 0.0;
-        for (int k = 0; k < 8; ++k) sum += red[(gg * 8 + k) * NPART + i];
-        partials[((long long)iy * nx + x0 + gg) * NPART + i] = sum;
-    }
-}

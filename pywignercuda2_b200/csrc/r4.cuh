@@ -103,9 +103,9 @@ template <class C> __device__ __forceinline__ void get(const C* s, const Lay& L,
 __device__ __forceinline__ void factor_mul(double2& v, double2 a, double2 b) { v = zmul(zmul(v, a), b); }
 __device__ __forceinline__ void factor_mul(float2& v, double2 a, double2 b) {
     float2 ah, al, bh, bl;
-    quad64::split_hl(a, ah, al);
-    quad64::split_hl(b, bh, bl);
-    v = quad64::fmul_hl(quad64::fmul_hl(v, ah, al), bh, bl);
+    ff::split_hl(a, ah, al);
+    ff::split_hl(b, bh, bl);
+    v = ff::fmul_hl(ff::fmul_hl(v, ah, al), bh, bl);
 }
 
 // one 32-byte sector: IL neighbouring planes' values of one point
@@ -125,7 +125,7 @@ __device__ __forceinline__ void st_sector(float2* p, const float2 (&v)[4]) {
 
 template <class C> __device__ __forceinline__ void make_tw(C* tw);
 template <> __device__ __forceinline__ void make_tw<double2>(double2* tw) { make_twiddles(tw, 64); }
-template <> __device__ __forceinline__ void make_tw<float2>(float2* tw) { quad64::make_norm_twiddles(tw); }
+template <> __device__ __forceinline__ void make_tw<float2>(float2* tw) { ff::make_norm_twiddles(tw); }
 
 }  // namespace r4
 
@@ -140,17 +140,10 @@ constexpr size_t r4_smem_bytes() { return sizeof(C) * (64 * 64 + 64) + sizeof(do
 // CL: launched as clusters of the IL planes f1 = IL m .. IL m + IL - 1 that
 // share each destination sector; the stores then go through distributed
 // shared memory so that every 32-byte sector is written whole (see the end).
-// PART: 0 the whole half-step; 1 its first half (load, forward transform,
-// factor), which stores the plane's frequencies from the L3 registers to
-// mid[plane][kr][kc] (whole lines); 2 its second half, which loads them back
-// into L3 and runs the inverse transform and the stores (and reductions).
-// The two halves move the state twice but each CTA does half the work per
-// byte, so loads and transforms of resident CTAs overlap better.
-template <class C, bool KIN, bool CL, int PART = 0>
+template <class C, bool KIN, bool CL>
 __global__ void __launch_bounds__(r4::NT, (sizeof(C) == 16 ? 2 : 4))
 k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__ PV, const C* __restrict__ gtw,
-     double2 scale, const double* __restrict__ d_norm, ObsTabs ob, double* __restrict__ partials,
-     C* __restrict__ mid) {
+     double2 scale, const double* __restrict__ d_norm, ObsTabs ob, double* __restrict__ partials) {
     using namespace r4;
     constexpr int IL = Il<C>::v, NQ = 64 / IL;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -159,15 +152,8 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
     double2* pvs = reinterpret_cast<double2*>(tw + 64);         // this plane's factor vectors
     const int t = threadIdx.x, pl = blockIdx.x, f0 = pl >> 6, f1 = pl & 63;
     const int ac = t & 15, ar = t >> 4;
-    // mid offset of register (i, j) in L3: kr = r2 + 4 r1 + 16 i, kc = c2 + 4 c1 + 16 j
-    const long long moff = (long long)pl * 4096 + ((t >> 6) + 4 * ((t >> 4) & 3)) * 64 + ((t >> 2) & 3) + 4 * (t & 3);
     C v[16];
-    if (PART == 2) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) v[4 * i + j] = mid[moff + i * 16 * 64 + j * 16];
-    } else {
+    {
         const C* g = src + ((((long long)ar * NQ + ac / IL) * 64 + f0) * 64 + f1) * IL + (ac % IL);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
@@ -176,12 +162,11 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
                 v[4 * i + j] = g[(long long)i * (16LL * 64 * 64 * 64) + (long long)j * (16LL * 64 * 64)];
     }
     if (t < 64) tw[t] = gtw[t];
-    if (PART != 2 && t < 128) pvs[t] = __ldg(PV + (long long)pl * 128 + t);
+    if (t < 128) pvs[t] = __ldg(PV + (long long)pl * 128 + t);
     double2 cc = scale;
     if (KIN && d_norm) cc = zmul(cc, zinv(make_double2(d_norm[0], d_norm[1])));
     const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
     __syncthreads();                                           // twiddles and factor vectors ready
-    if (PART != 2) {
     // ---- forward
     pass<C, true>(v);
     twiddle<C, true>(v, tw, ac, ar);
@@ -207,14 +192,6 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
 #pragma unroll
             for (int j = 0; j < 4; ++j) factor_mul(v[4 * i + j], a, b[j]);
         }
-    }
-    }  // PART != 2
-    if (PART == 1) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) mid[moff + i * 16 * 64 + j * 16] = v[4 * i + j];
-        return;
     }
     // ---- inverse
     pass<C, false>(v);
@@ -693,263 +670,4 @@ k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, PlaneSlots<C> S, const C
     r4t::fence_async_smem();                           // generic-proxy writes visible to the tensor store
     __syncthreads();
     if (threadIdx.x == 0) dpt::tma_store_4d(map, 2 * GP * m, 0, i1, 0, s);
-}
-
-// k_dplane_r4c: k_dplane_r4t with 32-byte box rows, half the rows per box.
-// A cluster of two CTAs takes the GPB = 32 B / sizeof(C) neighbouring planes
-// of one 32-byte piece (i3 = GPB m .. GPB m + GPB - 1).  CTA q loads the rows
-// i0 = 32 q .. 32 q + 31 of all GPB planes (box (2 GPB reals, 64, 1, 32),
-// 64 KB, stored as [i0 - 32 q][i2][plane]) and transforms the GP = GPB / 2
-// planes q GP + g, reading the other half of their rows from the partner's
-// box through distributed shared memory.  The results are staged back into
-// the two boxes the same way, and each CTA writes its box with one tensor
-// store.  Rows of a thread's points: ar + 16 i, so registers i = 0, 1 live in
-// CTA 0's box and i = 2, 3 in CTA 1's, for the load and for the staging.
-// A bounded wait that runs out does not leave early: both CTAs pass every
-// cluster barrier, the CTA skips its store, writes NaN into its first plane
-// and waits once more (bounded) for its copy.
-template <class C, bool FWD>
-__global__ void __launch_bounds__(r4::NT * dplane_gp<C>(), 2)
-k_dplane_r4c(const __grid_constant__ PlaneMaps<C> maps, PlaneSlots<C> S, const C* __restrict__ gtw, double2 scale,
-             const double* __restrict__ d_norm) {
-    using namespace r4;
-    namespace cg = cooperative_groups;
-    cg::cluster_group cl = cg::this_cluster();
-    constexpr int GP = dplane_gp<C>(), GPB = 2 * GP;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* s = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
-    C* tw = s + 4096 * GP;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(tw + 64);
-    const int t = threadIdx.x & 255, grp = threadIdx.x >> 8, ac = t & 15, ar = t >> 4;
-    const int q = (int)cl.block_rank(), pair = blockIdx.x >> 1;
-    const int i1 = pair / (64 / GPB), m = pair % (64 / GPB), pg = q * GP + grp;
-    const CUtensorMap* map = &maps.m[blockIdx.y];
-    if (threadIdx.x == 0) {
-        r4t::mbar_init(bar);
-        r4t::fence_async_smem();
-        r4t::mbar_expect_tx(bar, 65536);
-        dpt::tma_load_4d(s, map, 2 * GPB * m, 0, i1, 32 * q, bar);
-    }
-    if (threadIdx.x < 64) tw[threadIdx.x] = gtw[threadIdx.x];
-    double2 sc = scale;
-    if (d_norm) sc = zmul(sc, zinv(make_double2(d_norm[0], d_norm[1])));
-    const C cc = to_c<C>(sc);
-    C* box[2] = {cl.map_shared_rank(s, 0), cl.map_shared_rank(s, 1)};
-    __syncthreads();                                   // barrier initialised, twiddles ready
-    const bool ok = r4t::mbar_wait_bounded(bar);
-    cl.sync();                                         // both boxes in place
-    C v[16];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            v[4 * i + j] = box[i >> 1][((ar + 16 * (i & 1)) * 64 + ac + 16 * j) * GPB + pg];
-    if ((ar + ac) & 1) {
-#pragma unroll
-        for (int k = 0; k < 16; ++k) v[k] = cneg(v[k]);
-    }
-    C* sg = s + 4096 * grp;                            // this group's exchange plane
-    const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
-    cl.sync();                                         // both boxes have been read
-    pass<C, FWD>(v);
-    twiddle<C, FWD>(v, tw, ac, ar);
-    put(sg, L1, v);
-    __syncthreads();
-    get(sg, L2, v);
-    pass<C, FWD>(v);
-    twiddle<C, FWD>(v, tw, 4 * (t & 3), 4 * ((t >> 4) & 3));
-    __syncthreads();
-    put(sg, L2, v);
-    __syncthreads();
-    get(sg, L3, v);
-    pass<C, FWD>(v);
-    const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
-    const C ccs = ((r2 + c2) & 1) ? cneg(cc) : cc;
-    cl.sync();                                         // every exchange plane of both CTAs has been read
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            box[i >> 1][((r2 + 4 * r1 + 16 * (i & 1)) * 64 + c2 + 4 * c1 + 16 * j) * GPB + pg] =
-                cmul(v[4 * i + j], ccs);
-    asm volatile("fence.proxy.async;" ::: "memory");   // staged writes (local and remote) visible to the store
-    cl.sync();
-    if (threadIdx.x == 0) {
-        if (ok) {
-            dpt::tma_store_4d(map, 2 * GPB * m, 0, i1, 32 * q, s);
-        } else {
-            typedef typename real_of<C>::type R;
-            S.p[blockIdx.y][(long long)i1 * 64 * 64 + GPB * m + q * GP].x =
-                (R)__longlong_as_double(0x7ff8000000000000LL);
-            r4t::mbar_wait_bounded(bar);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// k_r4p: k_r4 as a persistent kernel that overlaps each plane's transforms
-// with the load of its next plane.
-//
-// A CTA loops over the planes blockIdx.x + k * gridDim.x with two plane
-// buffers B0, B1 in shared memory.  At iteration k the plane is in B[k&1]
-// (copied there by cp.async during iteration k-1, straight from global
-// memory without passing through registers); the thread reads its 16 points,
-// issues the copies of the next plane (and its factor vectors) into
-// B[(k+1)&1], and then uses B[k&1] for the four exchanges, the reduction and
-// the cluster staging.  B[(k+1)&1] is free at that moment: its last readers,
-// the partner CTAs of the previous iteration's cluster stores, finished
-// before that iteration's final cluster barrier.  Clusters keep their IL
-// CTAs on the same quad of planes because gridDim.x and the plane count are
-// multiples of IL.
-// ---------------------------------------------------------------------------
-template <class C>
-constexpr size_t r4p_smem_bytes() { return sizeof(C) * (2 * 64 * 64 + 64) + sizeof(double2) * 2 * 128; }
-
-template <class C, bool KIN>
-__global__ void __launch_bounds__(r4::NT, (sizeof(C) == 16 ? 1 : 3))
-k_r4p(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__ PV, const C* __restrict__ gtw,
-      double2 scale, const double* __restrict__ d_norm, ObsTabs ob, double* __restrict__ partials) {
-    using namespace r4;
-    namespace cg = cooperative_groups;
-    constexpr int IL = Il<C>::v, NQ = 64 / IL, NP = 64 * 64;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* buf0 = reinterpret_cast<C*>(smraw);
-    C* tw = buf0 + 2 * 64 * 64;
-    double2* pvb = reinterpret_cast<double2*>(tw + 64);        // [2][128]
-    const int t = threadIdx.x, ac = t & 15, ar = t >> 4;
-    cg::cluster_group cl = cg::this_cluster();
-    const int q = (int)cl.block_rank();
-    // this thread's 16 points of plane (f0, f1): src offsets relative to the plane base
-    auto prefetch = [&](int pl, int b) {
-        const int f0 = pl >> 6, f1 = pl & 63;
-        const C* g = src + ((((long long)ar * NQ + ac / IL) * 64 + f0) * 64 + f1) * IL + (ac % IL);
-        C* d = buf0 + b * 64 * 64;
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                cp_async_elem(d + (ar + 16 * i) * 64 + ac + 16 * j,
-                              g + (long long)i * (16LL * 64 * 64 * 64) + (long long)j * (16LL * 64 * 64));
-        if (t < 128)
-            cp_async_elem(pvb + b * 128 + t, PV + (long long)pl * 128 + t);
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    };
-    if (t < 64) tw[t] = gtw[t];
-    double2 cc = scale;
-    if (KIN && d_norm) cc = zmul(cc, zinv(make_double2(d_norm[0], d_norm[1])));
-    const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
-    if (blockIdx.x < NP) prefetch(blockIdx.x, 0);
-    int k = 0;
-    for (int pl = blockIdx.x; pl < NP; pl += gridDim.x, ++k) {
-        const int cur = k & 1, f0 = pl >> 6, f1 = pl & 63;
-        C* s = buf0 + cur * 64 * 64;
-        const double2* pvs = pvb + cur * 128;
-        cp_async_wait_all();
-        __syncthreads();                                     // plane, factor vectors (and twiddles) in place
-        C v[16];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) v[4 * i + j] = s[(ar + 16 * i) * 64 + ac + 16 * j];
-        if (pl + (int)gridDim.x < NP) prefetch(pl + gridDim.x, cur ^ 1);
-        // ---- forward
-        pass<C, true>(v);
-        twiddle<C, true>(v, tw, ac, ar);
-        __syncthreads();                                     // the plane has been read
-        put(s, L1, v);
-        __syncthreads();
-        get(s, L2, v);
-        pass<C, true>(v);
-        twiddle<C, true>(v, tw, 4 * (t & 3), 4 * ((t >> 4) & 3));
-        __syncthreads();
-        put(s, L2, v);
-        __syncthreads();
-        get(s, L3, v);
-        pass<C, true>(v);
-        {
-            const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
-            double2 b[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = pvs[64 + c2 + 4 * c1 + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const double2 a = zmul(pvs[r2 + 4 * r1 + 16 * i], cc);
-#pragma unroll
-                for (int j = 0; j < 4; ++j) factor_mul(v[4 * i + j], a, b[j]);
-            }
-        }
-        // ---- inverse
-        pass<C, false>(v);
-        twiddle<C, false>(v, tw, ((t >> 2) & 3) + 4 * (t & 3), (t >> 6) + 4 * ((t >> 4) & 3));
-        __syncthreads();
-        put(s, L3, v);
-        __syncthreads();
-        get(s, L2, v);
-        pass<C, false>(v);
-        twiddle<C, false>(v, tw, 4 * ((t >> 2) & 3), 4 * (t >> 6));
-        __syncthreads();
-        put(s, L2, v);
-        __syncthreads();
-        get(s, L1, v);
-        pass<C, false>(v);
-        if (!KIN) {
-            typedef typename real_of<C>::type R;
-            R a[NPART];
-#pragma unroll
-            for (int m = 0; m < NPART; ++m) a[m] = 0;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const R qy = (R)__ldg(ob.cpy + ar + 16 * i);
-                R w0x = 0, w0y = 0;
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const C w = v[4 * i + j];
-                    const R qx = (R)__ldg(ob.cpx + ac + 16 * j), kk = (R)__ldg(ob.ep + (ar + 16 * i) * 64 + ac + 16 * j);
-                    w0x += w.x; w0y += w.y;
-                    a[2] += qx * w.x; a[3] += qx * w.y;
-                    a[4] += qx * qx * w.x; a[5] += qx * qx * w.y;
-                    a[10] += kk * w.x; a[11] += kk * w.y;
-                }
-                a[0] += w0x; a[1] += w0y;
-                a[6] += qy * w0x; a[7] += qy * w0y;
-                a[8] += qy * qy * w0x; a[9] += qy * qy * w0y;
-            }
-            double* red = reinterpret_cast<double*>(s);
-            __syncthreads();                                 // last exchange read
-#pragma unroll
-            for (int m = 0; m < NPART; ++m) red[m * NT + t] = (double)a[m];
-            __syncthreads();
-            const int w = t >> 5, l = t & 31;
-            for (int m = w; m < NPART; m += NT / 32) {
-                double sum = 0.0;
-#pragma unroll
-                for (int u = 0; u < NT / 32; ++u) sum += red[m * NT + u * 32 + l];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
-                if (l == 0) partials[(long long)pl * NPART + m] = sum;
-            }
-        }
-        // ---- cluster stores (as k_r4): stage, gather the IL planes, whole sectors
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) s[(ar + 16 * i) * 64 + ac + 16 * j] = v[4 * i + j];
-        cl.sync();
-        const C* part[IL];
-#pragma unroll
-        for (int g = 0; g < IL; ++g) part[g] = cl.map_shared_rank(s, g);
-        C* gb = dst + ((long long)f0 * NQ + f1 / IL) * 64 * 64 * IL;
-        constexpr int PER = 4096 / IL / NT;
-#pragma unroll
-        for (int m = 0; m < PER; ++m) {
-            const int pt = q * (4096 / IL) + m * NT + t;
-            C val[IL];
-#pragma unroll
-            for (int g = 0; g < IL; ++g) val[g] = part[g][pt];
-            st_sector(gb + (long long)pt * IL, val);
-        }
-        cl.sync();                                           // partners done reading this buffer
-    }
-    cp_async_wait_all();
 }

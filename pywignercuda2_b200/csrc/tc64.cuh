@@ -156,16 +156,6 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t&
     lo = h2u(__floats2half2_rn(__fsub_rn(a, ah), __fsub_rn(b, bh)));
 }
 
-// float-float complex product v * (f_hi + f_lo)
-__device__ __forceinline__ float2 cmul_ff(float2 v, float2 fh, float2 fl) {
-    const float2 a = make_float2(v.x * fl.x - v.y * fl.y, v.x * fl.y + v.y * fl.x);
-    return make_float2(fmaf(v.x, fh.x, fmaf(-v.y, fh.y, a.x)), fmaf(v.x, fh.y, fmaf(v.y, fh.x, a.y)));
-}
-__device__ __forceinline__ void split_ff(double2 f, float2& h, float2& l) {
-    h = make_float2((float)f.x, (float)f.y);
-    l = make_float2((float)(f.x - (double)h.x), (float)(f.y - (double)h.y));
-}
-
 // Largest |value| of the pair (256 threads): each thread passes its own
 // maximum (non-negative); returns the power-of-two exponent e with
 // max * 2^-e in [2^14, 2^15) (-OP_EXP for an all-zero pair).
@@ -251,7 +241,7 @@ k_tc64(const float2* __restrict__ src, float2* __restrict__ dst, const double2* 
         // row factor vectors of the unit as float-float (used after stage 2)
         if (tp < 128) {
             float2 h, l;
-            split_ff(__ldg(PV + (long long)(plane0 + (tp >> 6)) * 128 + (tp & 63)), h, l);
+            ff::split_hl(__ldg(PV + (long long)(plane0 + (tp >> 6)) * 128 + (tp & 63)), h, l);
             pvs[tp] = make_float4(h.x, h.y, l.x, l.y);
         }
         int E;
@@ -315,12 +305,12 @@ k_tc64(const float2* __restrict__ src, float2* __restrict__ dst, const double2* 
             if (st == 2) {
                 // factor a(kr) b(kc) as float-float products; this thread's kc = ii
                 float2 bh, bl;
-                split_ff(__ldg(PV + (long long)(plane0 + p) * 128 + 64 + ii), bh, bl);
+                ff::split_hl(__ldg(PV + (long long)(plane0 + p) * 128 + 64 + ii), bh, bl);
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const float4 a = pvs[p * 64 + 32 * hf + j];
-                    float2 w = cmul_ff(make_float2(v[j], v[32 + j]), bh, bl);
-                    w = cmul_ff(w, make_float2(a.x, a.y), make_float2(a.z, a.w));
+                    float2 w = ff::fmul_hl(make_float2(v[j], v[32 + j]), bh, bl);
+                    w = ff::fmul_hl(w, make_float2(a.x, a.y), make_float2(a.z, a.w));
                     v[j] = w.x;
                     v[32 + j] = w.y;
                 }

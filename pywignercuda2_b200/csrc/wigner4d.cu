@@ -32,7 +32,6 @@
 
 #include "common.cuh"
 #include "fft_smem.cuh"
-#include "lanes64.cuh"
 
 void* wig_dense_matrix(int n, double delta, int dtype, cudaStream_t st);
 
@@ -406,154 +405,13 @@ __global__ void __launch_bounds__(256, (PotCfg<C, NPY, NPX, G>::MINB)) k_potenti
 }
 
 // ---------------------------------------------------------------------------
-// Run() kernels for 64 x 64 x 64 x 64 grids: register-resident transforms
-// (lanes64.cuh) and a ping-pong layout between the two half-steps.
+// Per-plane factor vectors of the 64^4 Run() kernels.
 //
-//   k_kin64: reads W in the reference layout L0 = [p_y][y][p_x][x] (each
-//            (y, x) plane is 64 rows of 1 KB), writes T in the transposed
-//            layout L1 = [y][x][p_y][p_x];
-//   k_pot64: reads T (each (p_y, p_x) plane is one contiguous 64 KB block),
-//            writes W in L0 and the partial sums of the observables.
-// Every global load is a contiguous 128-byte run per 8 lanes; the stores
-// are 16-byte (8-byte) scatters whose sectors are completed in L2 by the
-// CTAs of the neighbouring planes, which run at the same time.
-// ---------------------------------------------------------------------------
-template <class C>
-__global__ void __launch_bounds__(lanes64::NT, 2) k_kin64(const C* __restrict__ W, C* __restrict__ T,
-                                                          int npy, int npx, const __grid_constant__ FactorSet<C> F, double2 scale,
-                                                          const double* __restrict__ d_norm) {
-    using namespace lanes64;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* s = reinterpret_cast<C*>(smraw);
-    C* tw = s + 64 * LD;
-    const int tid = threadIdx.x, grp = tid >> 3, q = tid & 7, gi = grp & 3;
-    C* ws = s + (tid >> 5) * 4 * LD;
-    const int ipx = blockIdx.x % npx, ipy = blockIdx.x / npx;
-    make_twiddles(tw, 64);
-    const C* src = W + (((long long)ipy * 64 + grp) * npx + ipx) * 64;
-    C v[8];
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const C t = src[q + 8 * r];
-        v[r] = ((grp + q) & 1) ? cneg(t) : t;   // x = q + 8 r: parity of x + y is that of q + grp
-    }
-    double2 c0 = scale;
-    if (d_norm) c0 = zmul(c0, zinv(make_double2(d_norm[0], d_norm[1])));
-    const C cc = to_c<C>(c0);
-    __syncthreads();
-    fft64<C, true>(v, ws, gi, q, tw);                 // along x: v[k2] = (y = grp, kx = q + 8 k2)
-#pragma unroll
-    for (int k = 0; k < 8; ++k) s[grp * LD + q + 8 * k] = v[k];
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < 8; ++r) v[r] = s[(q + 8 * r) * LD + grp];
-    __syncthreads();
-    fft64<C, true>(v, ws, gi, q, tw);                 // along y: v[k2] = (ky = q + 8 k2, kx = grp)
-    const long long lin0 = ((long long)ipy * 64 * npx + ipx) * 64 + grp;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int ky = q + 8 * k;
-        v[k] = cmul(v[k], factor_at(F, ipy, ky, ipx, grp, lin0 + (long long)ky * npx * 64, cc));
-    }
-    fft64<C, false>(v, ws, gi, q, tw);                // v[k2] = (y = q + 8 k2, kx = grp)
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 8; ++k) s[(q + 8 * k) * LD + grp] = v[k];
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < 8; ++r) v[r] = s[grp * LD + q + 8 * r];
-    __syncthreads();
-    fft64<C, false>(v, ws, gi, q, tw);                // v[k2] = (y = grp, x = q + 8 k2)
-    C* dst = T + ((long long)grp * 64 * npy + ipy) * npx + ipx;
-    const long long xs = (long long)npy * npx;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int x = q + 8 * k;
-        dst[x * xs] = ((grp + x) & 1) ? cneg(v[k]) : v[k];
-    }
-}
-
-template <class C>
-__global__ void __launch_bounds__(lanes64::NT, 2) k_pot64(const C* __restrict__ T, C* __restrict__ W,
-                                                          int ny, int nx, const __grid_constant__ FactorSet<C> F, double2 scale,
-                                                          ObsTabs ob, double* __restrict__ partials) {
-    using namespace lanes64;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* s = reinterpret_cast<C*>(smraw);
-    C* tw = s + 64 * LD;
-    const int tid = threadIdx.x, grp = tid >> 3, q = tid & 7, gi = grp & 3;
-    C* ws = s + (tid >> 5) * 4 * LD;
-    const int ix = blockIdx.x % nx, iy = blockIdx.x / nx;
-    make_twiddles(tw, 64);
-    const C* src = T + ((long long)blockIdx.x * 64 + grp) * 64;   // row p_y = grp
-    C v[8];
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const C t = src[q + 8 * r];
-        v[r] = ((grp + q) & 1) ? cneg(t) : t;   // x = q + 8 r: parity of x + y is that of q + grp
-    }
-    const C cc = to_c<C>(scale);
-    __syncthreads();
-    fft64<C, true>(v, ws, gi, q, tw);                 // along p_x
-#pragma unroll
-    for (int k = 0; k < 8; ++k) s[grp * LD + q + 8 * k] = v[k];
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < 8; ++r) v[r] = s[(q + 8 * r) * LD + grp];
-    __syncthreads();
-    fft64<C, true>(v, ws, gi, q, tw);                 // along p_y: (theta_y = q + 8 k2, theta_x = grp)
-    const long long pys = (long long)ny * 64 * nx;
-    const long long lin0 = ((long long)iy * 64 + grp) * nx + ix;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int ky = q + 8 * k;
-        v[k] = cmul(v[k], factor_at(F, ky, iy, grp, ix, lin0 + ky * pys, cc));
-    }
-    fft64<C, false>(v, ws, gi, q, tw);
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 8; ++k) s[(q + 8 * k) * LD + grp] = v[k];
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < 8; ++r) v[r] = s[grp * LD + q + 8 * r];
-    __syncthreads();
-    fft64<C, false>(v, ws, gi, q, tw);                // (p_y = grp, p_x = q + 8 k2)
-    C* dst = W + (long long)grp * pys + (long long)iy * 64 * nx + ix;
-    double a[NPART];
-#pragma unroll
-    for (int i = 0; i < NPART; ++i) a[i] = 0.0;
-    const double qy = __ldg(ob.cpy + grp);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int px = q + 8 * k;
-        const C val = ((grp + px) & 1) ? cneg(v[k]) : v[k];
-        dst[(long long)px * nx] = val;
-        const double2 w = to_d2(val);
-        const double qx = __ldg(ob.cpx + px), kk = __ldg(ob.ep + grp * 64 + px);
-        a[0] += w.x; a[1] += w.y;
-        a[2] = fma(qx, w.x, a[2]); a[3] = fma(qx, w.y, a[3]);
-        a[4] = fma(qx * qx, w.x, a[4]); a[5] = fma(qx * qx, w.y, a[5]);
-        a[6] = fma(qy, w.x, a[6]); a[7] = fma(qy, w.y, a[7]);
-        a[8] = fma(qy * qy, w.x, a[8]); a[9] = fma(qy * qy, w.y, a[9]);
-        a[10] = fma(kk, w.x, a[10]); a[11] = fma(kk, w.y, a[11]);
-    }
-    __syncthreads();
-    block_sum_partials<NT>(a, reinterpret_cast<double*>(smraw), partials + (long long)blockIdx.x * NPART);
-}
-
-// ---------------------------------------------------------------------------
-// Persistent versions (one CTA of 512 threads per SM, looping over planes).
-//
-// * The next plane's global loads are issued into registers before the
-//   current plane is transformed, so they are in flight during the compute.
-// * No centring sign flips: with S = (-1)^(x+y), S IFFT2(F FFT2(S w)) equals
-//   IFFT2(F' FFT2(w)) where F'[k] = F[k + N/2] (indices mod N), so the factor
-//   is simply read at frequencies shifted by N/2.
-// * The factor of a plane is the product of per-plane vectors along each
-//   in-plane axis (built once per plane in shared memory from the pairwise
-//   tables) times, only if present, tables over both in-plane axes.
-// * k_pot64p accumulates every observable sum (11 complex) per thread over
-//   all of its planes; one partial row per CTA.
+// * No centring sign flips in the radix kernels: with S = (-1)^(x+y),
+//   S IFFT2(F FFT2(S w)) equals IFFT2(F' FFT2(w)) where F'[k] = F[k + N/2]
+//   (indices mod N), so the factor is read at frequencies shifted by N/2.
+// * The factor of a plane is the product of a vector along each in-plane
+//   axis, built once per plan from the pairwise tables.
 // ---------------------------------------------------------------------------
 #define NSUM 22   // sum W, xW, x^2 W, p_x W, p_x^2 W, yW, y^2 W, p_y W, p_y^2 W, K W, V W (complex)
 #define FOLD_BLOCKS 64   // first-stage rows of the Run() reduction over columns
@@ -590,172 +448,7 @@ __global__ void k_plane_vectors(const __grid_constant__ FactorSet<C> F, int ay, 
     PV[t] = to_c<C>(acc);
 }
 
-// 32-byte store of two adjacent complex values (one full sector for c128)
-__device__ __forceinline__ void st_pair(double2* p, double2 a, double2 b) {
-    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y)
-                 : "memory");
-}
-__device__ __forceinline__ void st_pair(float2* p, float2 a, float2 b) {
-    asm volatile("st.global.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y)
-                 : "memory");
-}
-
-// The two half-steps share one body: a CTA loops over PAIRS of planes that
-// are neighbours in the destination's fastest index, transforms both, and
-// writes each destination point pair with one 32-byte store.
-//   KIN: src plane (p_y, p_x) of W (L0), dst T (L1 = [y][x][p_y][p_x]);
-//   POT: src plane (y, x) of T (contiguous), dst W (L0), plus observables.
-template <class C, bool KIN>
-__device__ __forceinline__ const C* half64_src_row(const C* base, int pl, int n_f1, int grp) {
-    if (KIN) return base + (((long long)(pl / n_f1) * 64 + grp) * n_f1 + pl % n_f1) * 64;
-    return base + ((long long)pl * 64 + grp) * 64;
-}
-
-template <class C, bool KIN>
-__global__ void __launch_bounds__(lanes64::NT, 1) k_half64(const C* __restrict__ src_base, C* __restrict__ dst_base,
-                                                           int n_f0, int n_f1, const C* __restrict__ PV,
-                                                           double2 scale, const double* __restrict__ d_norm,
-                                                           ObsTabs ob, double* __restrict__ partials) {
-    using namespace lanes64;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* s = reinterpret_cast<C*>(smraw);
-    C* tw = s + 64 * LD;
-    C* fv = tw + 64;                 // 128: row vector then column vector of the plane
-    C* hold = fv + 128;              // results of the first plane of a pair [k][tid]
-    double* red = reinterpret_cast<double*>(hold + 8 * lanes64::NT);   // POT: [12][NT] per-plane partials
-    double* acc = red + 12 * lanes64::NT + 16;                            // POT: NSUM running sums
-    const int tid = threadIdx.x, grp = tid >> 3, q = tid & 7, gi = grp & 3;
-    C* ws = s + (tid >> 5) * 4 * LD;
-    const int nplanes = n_f0 * n_f1, npairs = nplanes >> 1;
-    make_twiddles(tw, 64);
-    double2 c0 = scale;
-    if (KIN && d_norm) c0 = zmul(c0, zinv(make_double2(d_norm[0], d_norm[1])));
-    const C cc = to_c<C>(c0);
-    // source row of plane pl for this thread: KIN -> W[((f0*64 + grp)*n_f1 + f1)*64 + x]
-    //                                         POT -> T[(pl*64 + grp)*64 + p_x]
-    if (!KIN && tid < NSUM) acc[tid] = 0.0;
-    int pair = blockIdx.x;
-    C nv[8];
-    C nf = mk<C>(0, 0);
-    if (pair < npairs) {
-        const C* r = half64_src_row<C, KIN>(src_base, 2 * pair, n_f1, grp);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) nv[i] = r[q + 8 * i];
-        if (tid < 128) nf = PV[(long long)(2 * pair) * 128 + tid];
-    }
-    for (; pair < npairs; pair += gridDim.x) {
-#pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-            const int pl = 2 * pair + h;
-            C v[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) v[i] = nv[i];
-            const C cur_f = nf;
-            const int next = h == 0 ? pl + 1 : 2 * (pair + gridDim.x);
-            if (next < nplanes) {
-                const C* r = half64_src_row<C, KIN>(src_base, next, n_f1, grp);
-#pragma unroll
-                for (int i = 0; i < 8; ++i) nv[i] = r[q + 8 * i];
-                if (tid < 128) nf = PV[(long long)next * 128 + tid];
-            }
-            const int f0 = pl / n_f1, f1 = pl % n_f1;
-            __syncthreads();                              // previous plane done with smem
-            if (tid < 128) fv[tid] = cur_f;
-            fft64<C, true>(v, ws, gi, q, tw);             // rows: (row = grp, kcol = q + 8 k)
-#pragma unroll
-            for (int k = 0; k < 8; ++k) s[grp * LD + q + 8 * k] = v[k];
-            __syncthreads();
-#pragma unroll
-            for (int r = 0; r < 8; ++r) v[r] = s[(q + 8 * r) * LD + grp];
-            __syncthreads();
-            fft64<C, true>(v, ws, gi, q, tw);             // columns: (krow = q + 8 k, kcol = grp)
-            const C fx = cmul(fv[64 + grp], cc);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = cmul(v[k], cmul(fv[q + 8 * k], fx));
-            fft64<C, false>(v, ws, gi, q, tw);
-            __syncthreads();
-#pragma unroll
-            for (int k = 0; k < 8; ++k) s[(q + 8 * k) * LD + grp] = v[k];
-            __syncthreads();
-#pragma unroll
-            for (int r = 0; r < 8; ++r) v[r] = s[grp * LD + q + 8 * r];
-            __syncthreads();
-            fft64<C, false>(v, ws, gi, q, tw);            // (row = grp, col = q + 8 k)
-            if (!KIN) {
-                // observables of the new (x, p) state (rows p_y = grp, columns p_x):
-                // per-thread partials -> smem -> 12 warps reduce one double each
-                // in a fixed order -> running sums with the plane's x, y, V(x, y)
-                double sw0 = 0.0, sw1 = 0.0, sx0 = 0.0, sx1 = 0.0, sxx0 = 0.0, sxx1 = 0.0, sk0 = 0.0, sk1 = 0.0;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int px = q + 8 * k;
-                    const double2 w = to_d2(v[k]);
-                    const double qx = __ldg(ob.cpx + px), kk = __ldg(ob.ep + grp * 64 + px);
-                    sw0 += w.x; sw1 += w.y;
-                    sx0 = fma(qx, w.x, sx0); sx1 = fma(qx, w.y, sx1);
-                    sxx0 = fma(qx * qx, w.x, sxx0); sxx1 = fma(qx * qx, w.y, sxx1);
-                    sk0 = fma(kk, w.x, sk0); sk1 = fma(kk, w.y, sk1);
-                }
-                const double qy = __ldg(ob.cpy + grp);
-                red[0 * NT + tid] = sw0;            red[1 * NT + tid] = sw1;
-                red[2 * NT + tid] = qy * sw0;       red[3 * NT + tid] = qy * sw1;
-                red[4 * NT + tid] = qy * qy * sw0;  red[5 * NT + tid] = qy * qy * sw1;
-                red[6 * NT + tid] = sx0;            red[7 * NT + tid] = sx1;
-                red[8 * NT + tid] = sxx0;           red[9 * NT + tid] = sxx1;
-                red[10 * NT + tid] = sk0;           red[11 * NT + tid] = sk1;
-                __syncthreads();
-                const int w = tid >> 5, l = tid & 31;
-                if (w < 12) {
-                    double t = 0.0;
-#pragma unroll
-                    for (int i = 0; i < NT / 32; ++i) t += red[w * NT + i * 32 + l];
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-                    if (l == 0) red[12 * NT + w] = t;   // scratch slots after the partials... see acc below
-                }
-                __syncthreads();
-                if (tid < 2) {   // tid 0: real parts, tid 1: imaginary parts
-                    const double* P = red + 12 * NT;
-                    const double x = __ldg(ob.cx + f1), y = __ldg(ob.cy + f0), V = __ldg(ob.ex + f0 * n_f1 + f1);
-                    const double W0 = P[0 + tid], Wy = P[2 + tid], Wyy = P[4 + tid];
-                    const double Wx = P[6 + tid], Wxx = P[8 + tid], Wk = P[10 + tid];
-                    acc[0 + tid] += W0;                 // sum W
-                    acc[2 + tid] += x * W0;             // x W
-                    acc[4 + tid] += x * x * W0;         // x^2 W
-                    acc[6 + tid] += Wx;                 // p_x W
-                    acc[8 + tid] += Wxx;                // p_x^2 W
-                    acc[10 + tid] += y * W0;            // y W
-                    acc[12 + tid] += y * y * W0;        // y^2 W
-                    acc[14 + tid] += Wy;                // p_y W
-                    acc[16 + tid] += Wyy;               // p_y^2 W
-                    acc[18 + tid] += Wk;                // K W
-                    acc[20 + tid] += V * W0;            // V W
-                }
-            }
-            if (h == 0) {
-#pragma unroll
-                for (int k = 0; k < 8; ++k) hold[k * NT + tid] = v[k];
-            } else {
-                // destination of (row = grp, col = c) for the plane pair (f0, f1 - 1 .. f1)
-                //   KIN: T[((y*64 + x)*n_f0 + p_y)*n_f1 + p_x] with y = grp, x = c, p_y = f0, p_x = f1
-                //   POT: W[((p_y*n_f0 + y)*64 + p_x)*n_f1 + x] with p_y = grp, p_x = c, y = f0, x = f1
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int c = q + 8 * k;
-                    const long long di = KIN ? (((long long)grp * 64 + c) * n_f0 + f0) * n_f1 + (f1 - 1)
-                                             : (((long long)grp * n_f0 + f0) * 64 + c) * n_f1 + (f1 - 1);
-                    st_pair(dst_base + di, hold[k * NT + tid], v[k]);
-                }
-            }
-        }
-    }
-    if (!KIN) {
-        __syncthreads();
-        if (tid < NSUM) partials[(long long)blockIdx.x * NSUM + tid] = acc[tid];
-    }
-}
-
-// Finalize for k_half64<pot>'s partial rows: NSUM sums per row.  One warp
+// Finalize of NSUM-wide partial rows (k_fold_columns' output).  One warp
 // per sum: lanes stride over the rows, then a fixed shuffle tree.
 __global__ void __launch_bounds__(32 * NSUM) k_finalize_sums(const double* __restrict__ part, int nrows,
                                                             double dv_norm, double dv_obs, double* out,
@@ -793,7 +486,7 @@ __global__ void __launch_bounds__(32 * NSUM) k_finalize_sums(const double* __res
     }
 }
 
-#include "quad64.cuh"
+#include "ff.cuh"
 #include "dense_half.cuh"
 #include "r4.cuh"
 #include "tc64.cuh"
@@ -992,6 +685,36 @@ __global__ void k_init_gauss(C* W, int n0, int n1, int n2, int n3, ObsTabs ob, d
     }
 }
 
+// Two displaced Gaussians in superposition ("cat state") on the (x, theta)
+// grid [theta_y][y][theta_x][x], built from the wave function as
+// WignerDiracGaussian_ParticleUp_GPU builds its spinor (GPU_WignerDirac4D.py:
+// 939-968): W = psi(x - theta/2) conj(psi(x + theta/2)) with
+//   psi(x, y) = [g(x - x0 - ax, y - y0 - ay) + g(x - x0 + ax, y - y0 + ay)]
+//               exp(i (px0 x + py0 y)),   g(u, v) = exp(-(u^2 + v^2) / 2).
+// The theta -> p transform (Fourier_Theta_To_P) then gives the Wigner
+// function, negative in the interference region.
+template <class C>
+__global__ void k_init_cat(C* W, int n0, int n1, int n2, int n3, ObsTabs ob, double dty, double dtx, double x0,
+                           double y0, double px0, double py0, double ax, double ay) {
+    const long long tot = (long long)n0 * n1 * n2 * n3;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int i3 = i % n3, i2 = (i / n3) % n2, i1 = (i / ((long long)n3 * n2)) % n1;
+        const int i0 = i / ((long long)n3 * n2 * n1);
+        const double x = ob.cx[i3], y = ob.cy[i1];
+        const double tx = dtx * (i2 - n2 / 2), ty = dty * (i0 - n0 / 2);
+        auto psi = [&](double u, double v) {
+            const double g = exp(-0.5 * ((u - x0 - ax) * (u - x0 - ax) + (v - y0 - ay) * (v - y0 - ay))) +
+                             exp(-0.5 * ((u - x0 + ax) * (u - x0 + ax) + (v - y0 + ay) * (v - y0 + ay)));
+            double s, c;
+            sincos(px0 * u + py0 * v, &s, &c);
+            return make_double2(g * c, g * s);
+        };
+        const double2 a = psi(x - 0.5 * tx, y - 0.5 * ty), b = psi(x + 0.5 * tx, y + 0.5 * ty);
+        W[i] = to_c<C>(zmul(a, make_double2(b.x, -b.y)));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Plan
 // ---------------------------------------------------------------------------
@@ -1014,19 +737,14 @@ struct wig4d_plan {
     double* cur_norm;              // complex128 norm of the current state
     int* counter;                  // history row of the next finalize
     int* flag;                     // WIG_ERR_NONFINITE when seen
-    bool fast64;                   // 64^4 grid: Run() uses k_kin64 / k_pot64
+    bool fast64;                   // 64^4 grid with separable factors: Run() uses k_r4
     void* pingpong;                // second state buffer (layout [y][x][p_y][p_x])
     void* pv;                      // per-plane factor vectors of the two half-steps
-    bool quad64;                   // complex64 64^4 Run(): k_quad64 on the LA / LB layouts
     bool r4;                       // 64^4 Run(): k_r4 (16 points per thread) on its LA / LB layouts
     bool r4t;                      // complex128 64^4 Run(): k_r4 with TMA plane loads (k_r4t)
     bool r4_cluster;               // k_r4 launched as clusters with full-sector stores
-    bool r4p;                      // persistent k_r4p (next plane prefetched by cp.async)
-    bool r4split;                  // each k_r4 half-step as two launches (PART 1, 2) through mid
-    void* mid;                     // k_r4 split: the planes' frequencies between the two launches
     int dense_n;                   // > 0: general-delta half-steps fused (k_dense_half, N^4 grids)
     const void* dmat[4];           // FAFT matrices per axis (|delta|), when dense_n > 0
-    int r4p_grid;                  // its CTAs: SMs x resident CTAs, a multiple of the cluster size
     void* tw64;                    // k_r4 twiddle table (64 complex of the plan's dtype)
     double* fold;                  // k_fold_columns output: FOLD_BLOCKS rows of NSUM
     bool tc;                       // complex64 64^4 Run(): k_tc64 (tensor-core DFTs) on the LK / LP layouts
@@ -1148,17 +866,6 @@ static int launch_potential(wig4d_plan* p, C* W, double* partials, cudaStream_t 
     const int ny = p->shape[1], nx = p->shape[3];
     const unsigned grid = (unsigned)(ny * nx);
     const double2 sc = make_double2(p->pot_scale, 0.0);
-    // k_pot48 (48 x 48 planes in registers) is selectable with WIG_POT48; it
-    // runs one CTA of 512 / 1024 threads per SM and measured slower than
-    // k_potential_g (416 against 316 us at 48^4 complex128)
-    if (NPY == 48 && NPX == 48 && nx % pot48_g<C>() == 0 && getenv("WIG_POT48") && !getenv("WIG_NO_K48")) {
-        const size_t sm = pot48_smem_bytes<C>();
-        WIG_CUDA(cudaFuncSetAttribute(k_pot48<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_pot48<C><<<(unsigned)(ny * (nx / pot48_g<C>())), k48::NT * pot48_g<C>(), sm, st>>>(
-            W, ny, nx, pot_set<C>(p), sc, p->ob, partials);
-        WIG_LAUNCHED("k_pot48");
-        return WIG_OK;
-    }
 #define PCASE(a, b)                                                                      \
     if (NPY == a && NPX == b) {                                                          \
         if (launch_potential_g<C, a, b>(p, W, partials, st, sc)) return WIG_OK;           \
@@ -1274,7 +981,6 @@ static void free_plan(wig4d_plan* p) {
     cudaFree(p->partials);
     cudaFree(p->cur_norm);
     cudaFree(p->pingpong);
-    cudaFree(p->mid);
     cudaFree(p->pv);
     cudaFree(p->tw64);
     cudaFree(p->fold);
@@ -1480,29 +1186,20 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
                 p->shape[2] == 64 && p->shape[3] == 64 && separable(desc->kin, desc->n_kin, 1, 3) &&
                 separable(desc->pot, desc->n_pot, 0, 2) && getenv("WIG_NO_FAST64") == nullptr;
     if (p->fast64) {
+        // k_r4 on the LA / LB layouts: a ping-pong buffer, FP64 per-plane
+        // factor vectors (from FP64 copies of the host tables for a
+        // complex64 plan, which keeps only float32 tables), the twiddles
         if (cudaMalloc(&p->pingpong, (size_t)p->npts * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
-        const int sm = (int)(esz * (64 * lanes64::LD + 64 + 128 + 8 * lanes64::NT) + sizeof(double) * (12 * lanes64::NT + 16 + NSUM));
         const int npl_k = p->shape[0] * p->shape[2], npl_p = p->shape[1] * p->shape[3];
-        if (cudaMalloc(&p->pv, (size_t)(npl_k + npl_p) * 128 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+        if (cudaMalloc(&p->pv, (size_t)(npl_k + npl_p) * 128 * sizeof(double2)) != cudaSuccess) {
+            free_plan(p); return WIG_ERR_ALLOC;
+        }
+        double2* pv = (double2*)p->pv;
         if (desc->dtype == WIG_C128) {
-            cudaFuncSetAttribute(k_half64<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-            cudaFuncSetAttribute(k_half64<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-            double2* pv = (double2*)p->pv;
             k_plane_vectors<double2><<<(npl_k * 128 + 255) / 256, 256>>>(p->kin_d, 1, 3, 0, 2, p->shape[2], npl_k, pv, 32);
             k_plane_vectors<double2><<<(npl_p * 128 + 255) / 256, 256>>>(p->pot_d, 0, 2, 1, 3, p->shape[3], npl_p,
                                                                         pv + (size_t)npl_k * 128, 32);
         } else {
-            // complex64: k_quad64 takes FP64 plane vectors, built from FP64
-            // copies of the tables (the plan keeps only the float32 ones)
-            p->quad64 = true;
-            const int qsm = (int)quad64_smem_bytes();
-            cudaFuncSetAttribute(k_quad64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, qsm);
-            cudaFuncSetAttribute(k_quad64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, qsm);
-            cudaFree(p->pv);
-            p->pv = nullptr;
-            if (cudaMalloc(&p->pv, (size_t)(npl_k + npl_p) * 128 * sizeof(double2)) != cudaSuccess) {
-                free_plan(p); return WIG_ERR_ALLOC;
-            }
             long long n64 = 0;
             for (int i = 0; i < desc->n_kin; ++i) n64 += tab_elems(desc->kin[i]);
             for (int i = 0; i < desc->n_pot; ++i) n64 += tab_elems(desc->pot[i]);
@@ -1523,7 +1220,6 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
                 ok = ok && cudaMemcpy(t64 + o64, desc->pot[i].host_data, n * 16, cudaMemcpyHostToDevice) == cudaSuccess;
                 p64.data[i] = t64 + o64; o64 += n;
             }
-            double2* pv = (double2*)p->pv;
             if (ok) {
                 k_plane_vectors<double2><<<(npl_k * 128 + 255) / 256, 256>>>(k64, 1, 3, 0, 2, p->shape[2], npl_k, pv, 32);
                 k_plane_vectors<double2><<<(npl_p * 128 + 255) / 256, 256>>>(p64, 0, 2, 1, 3, p->shape[3], npl_p,
@@ -1534,10 +1230,10 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             if (!ok) { wig_set_cuda_error(cudaGetLastError(), "plane vectors"); free_plan(p); return WIG_ERR_CUDA; }
         }
         // k_r4 with cluster stores (default); WIG_FAST64_KERNEL = r4 (plain
-        // stores), r4t (complex128 TMA loads) or pair (k_half64 / k_quad64)
+        // stores) or r4t (complex128 TMA plane loads)
         const char* kern = getenv("WIG_FAST64_KERNEL");
-        p->r4 = !(kern && strcmp(kern, "pair") == 0);
-        if (p->r4 && desc->dtype == WIG_C128 && kern && strcmp(kern, "r4t") == 0) {
+        p->r4 = true;
+        if (desc->dtype == WIG_C128 && kern && strcmp(kern, "r4t") == 0) {
             // k_r4 with TMA plane loads: LA map of the ping-pong buffer now,
             // LB map of the caller's state at the first run
             int r;
@@ -1546,63 +1242,22 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             cudaFuncSetAttribute(k_r4t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4t_smem_bytes());
             cudaFuncSetAttribute(k_r4t<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4t_smem_bytes());
         }
-        if (p->r4) {
-            p->quad64 = false;
-            p->r4_cluster = !(kern && strcmp(kern, "r4") == 0);
-            if (cudaMalloc(&p->tw64, 64 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
-            if (cudaMalloc(&p->fold, FOLD_BLOCKS * NSUM * sizeof(double)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
-            p->r4p = kern && strcmp(kern, "r4p") == 0;
-            p->r4split = !p->r4p && getenv("WIG_R4_SPLIT") != nullptr;
-            if (p->r4split && cudaMalloc(&p->mid, (size_t)p->npts * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
-            if (p->r4p) {
-                const int psm = (int)(desc->dtype == WIG_C128 ? r4p_smem_bytes<double2>() : r4p_smem_bytes<float2>());
-                const int il = desc->dtype == WIG_C128 ? 2 : 4;
-                int occ = 0;
-                if (desc->dtype == WIG_C128) {
-                    cudaFuncSetAttribute(k_r4p<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm);
-                    cudaFuncSetAttribute(k_r4p<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm);
-                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_r4p<double2, false>, r4::NT, psm);
-                } else {
-                    cudaFuncSetAttribute(k_r4p<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm);
-                    cudaFuncSetAttribute(k_r4p<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm);
-                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_r4p<float2, false>, r4::NT, psm);
-                }
-                if (occ < 1) occ = 1;
-                p->r4p_grid = (wig_num_sms() * occ / il) * il;
-            }
-            if (desc->dtype == WIG_C128) k_make_r4_twiddles<double2><<<1, 64>>>((double2*)p->tw64);
-            else k_make_r4_twiddles<float2><<<1, 64>>>((float2*)p->tw64);
-            const int rsm = (int)(desc->dtype == WIG_C128 ? r4_smem_bytes<double2>() : r4_smem_bytes<float2>());
-            if (desc->dtype == WIG_C128) {
-                cudaFuncSetAttribute(k_r4<double2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<double2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<double2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<double2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<double2, true, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<double2, false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<double2, true, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<double2, false, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<double2, true, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<double2, false, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-            } else {
-                cudaFuncSetAttribute(k_r4<float2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<float2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<float2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<float2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<float2, true, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<float2, false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<float2, true, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<float2, false, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<float2, true, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-                cudaFuncSetAttribute(k_r4<float2, false, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
-            }
-        }
-        // the persistent kernels write one NSUM row per CTA
-        if ((size_t)wig_num_sms() * NSUM > (size_t)p->shape[1] * p->shape[3] * NPART) {
-            cudaFree(p->partials);
-            if (cudaMalloc(&p->partials, (size_t)wig_num_sms() * NSUM * sizeof(double)) != cudaSuccess) {
-                free_plan(p); return WIG_ERR_ALLOC;
-            }
+        p->r4_cluster = !(kern && strcmp(kern, "r4") == 0);
+        if (cudaMalloc(&p->tw64, 64 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+        if (cudaMalloc(&p->fold, FOLD_BLOCKS * NSUM * sizeof(double)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+        if (desc->dtype == WIG_C128) k_make_r4_twiddles<double2><<<1, 64>>>((double2*)p->tw64);
+        else k_make_r4_twiddles<float2><<<1, 64>>>((float2*)p->tw64);
+        const int rsm = (int)(desc->dtype == WIG_C128 ? r4_smem_bytes<double2>() : r4_smem_bytes<float2>());
+        if (desc->dtype == WIG_C128) {
+            cudaFuncSetAttribute(k_r4<double2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+            cudaFuncSetAttribute(k_r4<double2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+            cudaFuncSetAttribute(k_r4<double2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+            cudaFuncSetAttribute(k_r4<double2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+        } else {
+            cudaFuncSetAttribute(k_r4<float2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+            cudaFuncSetAttribute(k_r4<float2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+            cudaFuncSetAttribute(k_r4<float2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+            cudaFuncSetAttribute(k_r4<float2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
         }
     }
     // tensor-core transforms (k_tc64): complex64 64^4, separable factors,
@@ -1676,7 +1331,7 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     if (!p || !info) return WIG_ERR_INVALID_ARG;
     info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64;
-    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4p ? 5 : (p->r4t ? 4 : (p->r4 ? 3 : (p->quad64 ? 2 : 1)))));
+    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4t ? 4 : 3));
     return WIG_OK;
 }
 
@@ -1702,10 +1357,9 @@ static int launch_dplane_r4(void* const* slots, int nslots, const void* tw, doub
     return WIG_OK;
 }
 
-// 4-D view of one 64^4 component for k_dplane_r4t / k_dplane_r4c:
-// (2 * 64 reals, i2, i1, i0); box (reals, 64, 1, rows): (2 GP reals = 16
-// bytes, 64, 1, 64) for k_dplane_r4t, (4 GP reals = 32 bytes, 64, 1, 32) for
-// k_dplane_r4c.
+// 4-D view of one 64^4 component for k_dplane_r4t:
+// (2 * 64 reals, i2, i1, i0); box (reals, 64, 1, rows) = (2 GP reals = 16
+// bytes, 64, 1, 64).
 template <class C>
 static int encode_dplane_map(CUtensorMap* m, const void* base, int reals, int rows) {
     constexpr cuuint64_t E = sizeof(C);
@@ -1750,49 +1404,12 @@ static int launch_dplane_r4t(void* const* slots, int nslots, const void* tw, dou
     return WIG_OK;
 }
 
-template <class C, bool FWD>
-static int launch_dplane_r4c(void* const* slots, int nslots, const void* tw, double scale, const double* d_norm,
-                             cudaStream_t st) {
-    PlaneMaps<C> maps;
-    PlaneSlots<C> S;
-    memset(&maps, 0, sizeof(maps));
-    for (int k = 0; k < 16; ++k) S.p[k] = k < nslots ? (C*)slots[k] : nullptr;
-    constexpr int GP = dplane_gp<C>();
-    for (int k = 0; k < nslots; ++k) {
-        int r;
-        if ((r = encode_dplane_map<C>(&maps.m[k], slots[k], 4 * GP, 32))) return r;
-    }
-    auto kern = k_dplane_r4c<C, FWD>;
-    const size_t sm = dplane_r4t_smem_bytes<C>();
-    WIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(2 * 64 * 64 / (2 * GP), nslots);
-    cfg.blockDim = dim3(r4::NT * GP);
-    cfg.dynamicSmemBytes = sm;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = 2;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    WIG_CUDA(cudaLaunchKernelEx(&cfg, kern, maps, S, (const C*)tw, make_double2(scale, 0.0), d_norm));
-    return WIG_OK;
-}
-
 // kind 0: axes (1, 3), kind 1: axes (0, 2) of a 64^4 component; fwd: exp(-i ...)
 int wig_dplane64(void* const* slots, int nslots, int dtype, int kind, int fwd, double scale, const double* d_norm,
                  const void* tw, cudaStream_t st) {
     if (nslots < 1 || nslots > 16 || !tw) return WIG_ERR_INVALID_ARG;
     for (int k = 0; k < nslots; ++k)
         if (!slots[k] || (reinterpret_cast<uintptr_t>(slots[k]) & 15)) return WIG_ERR_INVALID_ARG;
-    if (kind == 1 && !getenv("WIG_NO_DPLANE_TMA") && getenv("WIG_DPLANE_CLUSTER")) {
-        if (dtype == WIG_C128) return fwd ? launch_dplane_r4c<double2, true>(slots, nslots, tw, scale, d_norm, st)
-                                          : launch_dplane_r4c<double2, false>(slots, nslots, tw, scale, d_norm, st);
-        return fwd ? launch_dplane_r4c<float2, true>(slots, nslots, tw, scale, d_norm, st)
-                   : launch_dplane_r4c<float2, false>(slots, nslots, tw, scale, d_norm, st);
-    }
     if (kind == 1 && !getenv("WIG_NO_DPLANE_TMA")) {
         if (dtype == WIG_C128) return fwd ? launch_dplane_r4t<double2, true>(slots, nslots, tw, scale, d_norm, st)
                                           : launch_dplane_r4t<double2, false>(slots, nslots, tw, scale, d_norm, st);
@@ -1816,7 +1433,7 @@ extern "C" long long wig4d_plan_device_bytes(const wig4d_plan* p) {
     const long long N0 = p->shape[0], N1 = p->shape[1], N2 = p->shape[2], N3 = p->shape[3];
     const long long esz = p->dtype == WIG_C128 ? 16 : 8;
     return p->tab_bytes + 8 * (N0 + N1 + N2 + N3 + N0 * N2 + N1 * N3) + 8LL * N1 * N3 * NPART + 32 +
-           (p->pingpong ? p->npts * esz : 0) + (p->mid ? p->npts * esz : 0);
+           (p->pingpong ? p->npts * esz : 0);
 }
 
 extern "C" int wig4d_kinetic(wig4d_plan* p, void* W, const double* d_norm, void* stream) {
@@ -1881,15 +1498,37 @@ static __device__ __align__(256) double g_noalloc_partials[(size_t)WIG4D_NOALLOC
 
 // Device address of g_noalloc_partials, looked up once per device with the
 // device current (in host code the symbol is only a stand-in, not an address).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+static CtxGetCurrentFn ctx_get_current_fn() {
+    static CtxGetCurrentFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(f);
+    });
+    return fn;
+}
+
+// The array's device address for the current device, looked up at the first
+// call on that device and again whenever the device's current context is not
+// the one of the cached address (after a device reset the old address would
+// point into freed memory).
 static double* noalloc_scratch(int* status) {
     static std::mutex mu;
     static double* addr[64] = {nullptr};
+    static CUcontext ctxs[64] = {nullptr};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) { wig_set_cuda_error(e, "cudaGetDevice"); *status = WIG_ERR_CUDA; return nullptr; }
     if (dev < 0 || dev >= 64) { *status = WIG_ERR_UNSUPPORTED; return nullptr; }
+    CUcontext ctx = nullptr;
+    const CtxGetCurrentFn get_ctx = ctx_get_current_fn();
+    if (get_ctx) get_ctx(&ctx);
     std::lock_guard<std::mutex> lk(mu);
-    if (!addr[dev]) {
+    if (!addr[dev] || ctxs[dev] != ctx || !get_ctx) {
         void* ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_noalloc_partials);
         if (e != cudaSuccess || !ptr) {
@@ -1898,6 +1537,7 @@ static double* noalloc_scratch(int* status) {
             return nullptr;
         }
         addr[dev] = static_cast<double*>(ptr);
+        ctxs[dev] = ctx;
     }
     *status = WIG_OK;
     return addr[dev];
@@ -1956,32 +1596,13 @@ static int fold_and_finalize(wig4d_plan* p, double* hist, int rows, cudaStream_t
     return WIG_OK;
 }
 
-// k_r4p launch: persistent, clusters of IL CTAs.
-template <class C, bool KIN>
-static cudaError_t launch_r4p(unsigned grid, cudaStream_t st, const C* src, C* dst, const double2* pv, const C* tw,
-                              double2 scale, const double* d_norm, ObsTabs ob, double* partials) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(r4::NT);
-    cfg.dynamicSmemBytes = r4p_smem_bytes<C>();
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = r4::Il<C>::v;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_r4p<C, KIN>, src, dst, pv, tw, scale, d_norm, ob, partials);
-}
-
 // k_r4 launch: with clusters of IL CTAs (full-sector stores) or plain.
 template <class C, bool KIN>
 static cudaError_t launch_r4(bool cluster, unsigned grid, size_t sm, cudaStream_t st, const C* src, C* dst,
                              const double2* pv, const C* tw, double2 scale, const double* d_norm, ObsTabs ob,
                              double* partials) {
     if (!cluster) {
-        k_r4<C, KIN, false><<<grid, r4::NT, sm, st>>>(src, dst, pv, tw, scale, d_norm, ob, partials, nullptr);
+        k_r4<C, KIN, false><<<grid, r4::NT, sm, st>>>(src, dst, pv, tw, scale, d_norm, ob, partials);
         return cudaGetLastError();
     }
     cudaLaunchConfig_t cfg = {};
@@ -1996,36 +1617,7 @@ static cudaError_t launch_r4(bool cluster, unsigned grid, size_t sm, cudaStream_
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_r4<C, KIN, true>, src, dst, pv, tw, scale, d_norm, ob, partials, (C*)nullptr);
-}
-
-// k_r4 as two launches: the first half (no clusters; whole-line stores to
-// mid), then the second half with the cluster stores of launch_r4.
-template <class C, bool KIN>
-static cudaError_t launch_r4_split(bool cluster, unsigned grid, size_t sm, cudaStream_t st, const C* src, C* dst,
-                                   const double2* pv, const C* tw, double2 scale, const double* d_norm, ObsTabs ob,
-                                   double* partials, C* mid) {
-    k_r4<C, KIN, false, 1><<<grid, r4::NT, sm, st>>>(src, nullptr, pv, tw, scale, d_norm, ob, nullptr, mid);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    if (!cluster) {
-        k_r4<C, KIN, false, 2><<<grid, r4::NT, sm, st>>>(nullptr, dst, pv, tw, scale, d_norm, ob, partials, mid);
-        return cudaGetLastError();
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(r4::NT);
-    cfg.dynamicSmemBytes = sm;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = r4::Il<C>::v;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_r4<C, KIN, true, 2>, (const C*)nullptr, dst, pv, tw, scale, d_norm, ob, partials,
-                              mid);
+    return cudaLaunchKernelEx(&cfg, k_r4<C, KIN, true>, src, dst, pv, tw, scale, d_norm, ob, partials);
 }
 
 template <class C>
@@ -2083,29 +1675,6 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
         const double2* pv = reinterpret_cast<const double2*>(p->pv);
         constexpr size_t sm = r4_smem_bytes<C>();
         const unsigned nplanes = 64 * 64;
-        if (p->r4p && part < 2) {
-            if (part == 0)
-                WIG_CUDA((launch_r4p<C, true>(p->r4p_grid, st, P, W, pv, (const C*)p->tw64,
-                                              make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr)));
-            else
-                WIG_CUDA((launch_r4p<C, false>(p->r4p_grid, st, W, P, pv + (size_t)p->shape[0] * p->shape[2] * 128,
-                                               (const C*)p->tw64, make_double2(p->pot_scale, 0.0), nullptr, p->ob,
-                                               p->partials)));
-            WIG_LAUNCHED("k_r4p");
-            return WIG_OK;
-        }
-        if (p->r4split && part < 2) {
-            C* M = reinterpret_cast<C*>(p->mid);
-            if (part == 0)
-                WIG_CUDA((launch_r4_split<C, true>(p->r4_cluster, nplanes, sm, st, P, W, pv, (const C*)p->tw64,
-                                                   make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr, M)));
-            else
-                WIG_CUDA((launch_r4_split<C, false>(p->r4_cluster, nplanes, sm, st, W, P,
-                                                    pv + (size_t)p->shape[0] * p->shape[2] * 128, (const C*)p->tw64,
-                                                    make_double2(p->pot_scale, 0.0), nullptr, p->ob, p->partials, M)));
-            WIG_LAUNCHED("k_r4 split");
-            return WIG_OK;
-        }
         if (part == 0) {
             WIG_CUDA((launch_r4<C, true>(p->r4_cluster, nplanes, sm, st, P, W, pv, (const C*)p->tw64,
                                          make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr)));
@@ -2117,50 +1686,6 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
             WIG_LAUNCHED("k_r4<pot>");
         } else {
             return fold_and_finalize(p, hist, rows, st);
-        }
-        return WIG_OK;
-    }
-    if constexpr (std::is_same<C, float2>::value) {
-        if (p->quad64) {
-            // W holds LB, the ping-pong buffer LA (converted around the loop)
-            float2* P = reinterpret_cast<float2*>(p->pingpong);
-            const double2* pv = reinterpret_cast<const double2*>(p->pv);
-            const int nsm = wig_num_sms();
-            constexpr size_t sm = quad64_smem_bytes();
-            if (part == 0) {
-                k_quad64<true><<<nsm, quad64::NT, sm, st>>>(P, W, p->shape[0], pv, make_double2(p->kin_scale, 0.0),
-                                                           p->cur_norm, p->ob, nullptr);
-                WIG_LAUNCHED("k_quad64<kin>");
-            } else if (part == 1) {
-                k_quad64<false><<<nsm, quad64::NT, sm, st>>>(W, P, p->shape[1], pv + (size_t)p->shape[0] * p->shape[2] * 128,
-                                                            make_double2(p->pot_scale, 0.0), nullptr, p->ob, p->partials);
-                WIG_LAUNCHED("k_quad64<pot>");
-            } else {
-                k_finalize_sums<<<1, 32 * NSUM, 0, st>>>(p->partials, nsm, p->dv_norm, p->dv_obs, hist, p->counter,
-                                                         rows, p->cur_norm, p->flag);
-                WIG_LAUNCHED("k_finalize_sums");
-            }
-            return WIG_OK;
-        }
-    }
-    if (p->fast64) {
-        constexpr size_t sm = sizeof(C) * (64 * lanes64::LD + 64 + 128 + 8 * lanes64::NT) + sizeof(double) * (12 * lanes64::NT + 16 + NSUM);
-        C* T = reinterpret_cast<C*>(p->pingpong);
-        const int nsm = wig_num_sms();
-        const C* pvk = reinterpret_cast<const C*>(p->pv);
-        const C* pvp = pvk + (size_t)p->shape[0] * p->shape[2] * 128;
-        if (part == 0) {
-            k_half64<C, true><<<nsm, lanes64::NT, sm, st>>>(W, T, p->shape[0], p->shape[2], pvk,
-                                                            make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr);
-            WIG_LAUNCHED("k_half64<kin>");
-        } else if (part == 1) {
-            k_half64<C, false><<<nsm, lanes64::NT, sm, st>>>(T, W, p->shape[1], p->shape[3], pvp,
-                                                             make_double2(p->pot_scale, 0.0), nullptr, p->ob, p->partials);
-            WIG_LAUNCHED("k_half64<pot>");
-        } else {
-            k_finalize_sums<<<1, 32 * NSUM, 0, st>>>(p->partials, nsm, p->dv_norm, p->dv_obs, hist, p->counter, rows,
-                                                     p->cur_norm, p->flag);
-            WIG_LAUNCHED("k_finalize_sums");
         }
         return WIG_OK;
     }
@@ -2194,9 +1719,6 @@ static int enter_loop_layout(wig4d_plan* p, void* W, cudaStream_t st) {
         WIG_LAUNCHED("k_to_r4_layout");
         return WIG_OK;
     }
-    if (!p->quad64) return WIG_OK;
-    k_to_quad_layout<<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)W, (float2*)p->pingpong, p->npts);
-    WIG_LAUNCHED("k_to_quad_layout");
     return WIG_OK;
 }
 
@@ -2220,11 +1742,7 @@ static int leave_loop_layout(wig4d_plan* p, void* W, cudaStream_t st, bool divid
         WIG_LAUNCHED("k_from_r4_layout");
         return WIG_OK;
     }
-    if (!p->quad64) return divide ? wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st) : WIG_OK;
-    k_from_quad_layout<<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)p->pingpong, (float2*)W, p->npts,
-                                                          divide ? p->cur_norm : nullptr);
-    WIG_LAUNCHED("k_from_quad_layout");
-    return WIG_OK;
+    return divide ? wig_divide_by_device_scalar(W, p->npts, p->dtype, p->cur_norm, st) : WIG_OK;
 }
 
 template <class C>
@@ -2420,6 +1938,23 @@ extern "C" int wig4d_init_ho_ground(wig4d_plan* p, void* W, double x_mu, double 
         k_init_ho<float2><<<grid_for(p->npts), 256, 0, st>>>((float2*)W, p->shape[0], p->shape[1], p->shape[2],
                                                             p->shape[3], p->ob, x_mu, y_mu, px_mu, py_mu, wx, wy, mass);
     WIG_LAUNCHED("k_init_ho");
+    return WIG_OK;
+}
+
+extern "C" int wig4d_init_cat_xtheta(wig4d_plan* p, void* W, double dtheta_y, double dtheta_x, double x_mu,
+                                    double y_mu, double p_x_mu, double p_y_mu, double a_x, double a_y,
+                                    void* stream) {
+    if (!p || !W) return WIG_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    if (p->dtype == WIG_C128)
+        k_init_cat<double2><<<grid_for(p->npts), 256, 0, st>>>((double2*)W, p->shape[0], p->shape[1], p->shape[2],
+                                                              p->shape[3], p->ob, dtheta_y, dtheta_x, x_mu, y_mu,
+                                                              p_x_mu, p_y_mu, a_x, a_y);
+    else
+        k_init_cat<float2><<<grid_for(p->npts), 256, 0, st>>>((float2*)W, p->shape[0], p->shape[1], p->shape[2],
+                                                             p->shape[3], p->ob, dtheta_y, dtheta_x, x_mu, y_mu,
+                                                             p_x_mu, p_y_mu, a_x, a_y);
+    WIG_LAUNCHED("k_init_cat");
     return WIG_OK;
 }
 

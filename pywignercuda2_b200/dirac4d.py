@@ -143,11 +143,22 @@ class GPU_WignerDirac4D:
         vm, vp = zy - 0.5 * ty[None, :], zy + 0.5 * ty[None, :]
         fields = []
         rank = 0
-        for k in (1, 2, 3):
-            for U, V in ((um, vm), (up, vp)):
-                F, G = lowrank.field_tables(lambda u, v, tree=A[k]: expr.evaluate(tree, t=0.0, x=u, y=v), U, V)
-                fields.append((F, G))
-                rank = max(rank, F.shape[0])
+        afull = None
+        try:
+            for k in (1, 2, 3):
+                for U, V in ((um, vm), (up, vp)):
+                    F, G = lowrank.field_tables(lambda u, v, tree=A[k]: expr.evaluate(tree, t=0.0, x=u, y=v), U, V)
+                    fields.append((F, G))
+                    rank = max(rank, F.shape[0])
+        except lowrank.RankError:
+            # not of low rank (e.g. exp(-(x-y)^2)): A at both Bopp sides on
+            # every point, [k][side][theta_y][y][theta_x][x]
+            fields, rank = [], 0
+            afull = np.empty((3, 2, N0, N1, N2, N3))
+            for k in (1, 2, 3):
+                for side, (U, V) in enumerate(((um, vm), (up, vp))):
+                    afull[k - 1, side] = np.broadcast_to(expr.evaluate(
+                        A[k], t=0.0, x=U.T[None, None, :, :], y=V.T[:, :, None, None]), (N0, N1, N2, N3))
         nu, nv = N3 * N2, N1 * N0
         atab = np.zeros((3, 2, max(rank, 1), nu + nv))
         for i, (F, G) in enumerate(fields):
@@ -156,6 +167,7 @@ class GPU_WignerDirac4D:
                 atab[k, side, r, :nu] = F[r].reshape(nu)
                 atab[k, side, r, nu:] = G[r].reshape(nv)
         self._a_rank = rank
+        self._a_full = afull is not None
 
         # A0 phase exp(-i dt (A0(x-) - A0(x+)) / hbar) on (theta_y, y, theta_x, x)
         def a0_phase(ty_, y_, tx_, x_):
@@ -213,6 +225,8 @@ class GPU_WignerDirac4D:
                 d.phase[i].axis_a, d.phase[i].axis_b, d.phase[i].host_data = a, b, _lib.dptr(arr)
         d.a_rank = rank
         d.a_tabs = dp(atab.reshape(-1))
+        if afull is not None:
+            d.a_full = dp(afull.reshape(-1))
         d.obs_xy = dp(obs.reshape(-1))
         d.dv_norm = self.dx * self.dp_x * self.dy * self.dp_y
         d.dv_obs = self._c("dx") * self._c("dy") * self._c("dp_x") * self._c("dp_y")

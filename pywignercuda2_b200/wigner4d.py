@@ -200,6 +200,19 @@ class GPU_Wigner4D:
         _lib.call("wig4d_init_gaussian", self._plan, self._check(W), mu_p_y, mu_y, mu_p_x, mu_x,
                   sigma_p_y, sigma_y, sigma_p_x, sigma_x, stream_ptr())
 
+    def CatState_GPU(self, W, x_mu, y_mu, p_x_mu, p_y_mu, a_x, a_y):
+        """Two displaced Gaussians in superposition (no reference initialiser):
+        the wave function psi = [g(q - q_mu - a) + g(q - q_mu + a)] exp(i p_mu . q),
+        g = exp(-|q|^2 / 2), turned into W(x, theta) = psi(x - theta/2)
+        conj(psi(x + theta/2)) on the device, then Fourier_Theta_To_P_GPU into
+        the (x, p) grid -- the pattern of WignerDiracGaussian_ParticleUp_GPU
+        and the notebooks' preparation (GPU_WignerDirac4D.py:939-968).  The
+        result is real up to rounding and negative where the two Gaussians
+        interfere; Run() normalises it."""
+        _lib.call("wig4d_init_cat_xtheta", self._plan, self._check(W), self._c("dtheta_y"), self._c("dtheta_x"),
+                  x_mu, y_mu, p_x_mu, p_y_mu, a_x, a_y, stream_ptr())
+        self.Fourier_Theta_To_P_GPU(W)
+
     def HOscillatorGound_GPU(self, W, x_mu, y_mu, p_x_mu, p_y_mu, omega_x, omega_y, mass):
         _lib.call("wig4d_init_ho_ground", self._plan, self._check(W), x_mu, y_mu, p_x_mu, p_y_mu,
                   omega_x, omega_y, mass, stream_ptr())
@@ -313,7 +326,7 @@ class GPU_Wigner4D:
         """Kernels the plan runs: fused_kinetic, fused_potential, fast64, run64_kernel."""
         info = (ctypes.c_int * 4)()
         _lib.call("wig4d_plan_info", self._plan, info)
-        run64 = {0: None, 1: "half64", 2: "quad64", 3: "r4", 4: "r4t", 5: "r4p", 6: "tc"}[info[3]]
+        run64 = {0: None, 3: "r4", 4: "r4t", 6: "tc"}[info[3]]
         return {"fused_kinetic": bool(info[0]), "fused_potential": bool(info[1]), "fast64": bool(info[2]),
                 "run64_kernel": run64}
 
@@ -370,7 +383,8 @@ class GPU_Wigner4D:
                       0 if last else _lib.WIG_RUN_KEEP_NORM, stream_ptr())
             h = hist.cpu().numpy()
             # the state that entered this chunk, normalised by its row-0 norm
-            self.snapshots.append((t * self.dt, self._snapshot_from(self._W0_copy, h[0])))
+            t0 = float(getattr(self, "time_offset", 0.0))
+            self.snapshots.append((t0 + t * self.dt, self._snapshot_from(self._W0_copy, h[0])))
             rows.append(h)
             t += n
             if not last:

@@ -83,4 +83,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the cabrer7/PyWignerCUDA2 checkout>")
+    main(sys.argv[1])

@@ -158,26 +158,63 @@ def test_run_parity(kvn, fast, alias, filt):
     assert err16(comps(f), o.W) < 1e-11
 
 
-def test_golden_x_notebook_on_gpu():
-    """instances/WignerDirac4D_64_64/X.ipynb: init norm 9065.39215134, then the
-    Run() norms 0.9999809946, 10.3216821369, 10.321709756 (mask constant 7)."""
-    name = "instances/WignerDirac4D_64_64/X.ipynb"
-    cfg = NOTEBOOKS[name]
-    f = make_frame(GPU_WignerDirac4D, cfg["params"], bound_p=7.0)
+def _prepare_gpu(f, cfg):
+    """The notebook's preparation on the GPU frame (the sequences of
+    tests/golden/notebook_configs.py); returns the printed norm."""
     Ws = all_w(f)
-    f.WignerDiracGaussian_ParticleUp_GPU(*Ws, 0.5, 0.0, 0.0, 0.0, 2.2, 2.2)
-    f._Fourier_Theta_To_P_64_64_4x4_GPU(*Ws)
-    f.boundary_p_GPU(*Ws)
+    kind = cfg["init"]
+    if kind == "landau":
+        f.WignerLandaoGround_GPU(*Ws, cfg["B"], 0.0, 0.0)
+    else:
+        ux, uy = cfg["u"]
+        f.WignerDiracGaussian_ParticleUp_GPU(*Ws, ux, uy, 0.0, 0.0, 2.2, 2.2)
+    if kind in ("up", "landau"):
+        f._Fourier_Theta_To_P_64_64_4x4_GPU(*Ws)
+        f.boundary_p_GPU(*Ws)
+    else:
+        f.Fourier_Theta_To_P_64_64_4x4_GPU(*Ws)
+        f.Fourier_X_To_Lambda_64_64_4x4_GPU(*Ws)
+        if kind == "filtered":
+            f.ParticleProjector_GPU(*Ws, 1)
+        f.Fourier_Lambda_To_X_64_64_4x4_GPU(*Ws)
     for k in (0, 5, 10, 15):
         f.Real_GPU(Ws[k])
-    n0 = f.Normalize_4x4_GPU(*Ws)
-    g = GOLD[name]
-    assert abs(n0.real - g["init_norms"][0]) < 1e-11 * g["init_norms"][0]
-    f.timeSteps = 2
+    return f.Normalize_4x4_GPU(*Ws)
+
+
+OTHER_REVISION = {"instances/WignerDirac4D_64_64/Free.ipynb", "instances/WignerDirac4D_64_64/X2.ipynb",
+                  "instances/WignerDirac4D_64_64/FreeFiltered.ipynb",
+                  "instances/WignerDirac4D_64_64/SternGerlach.ipynb"}
+
+
+@pytest.mark.parametrize("name", sorted(NOTEBOOKS))
+def test_golden_notebook_init_norm_on_gpu(name):
+    """Every notebook's printed initial trace norm (12 digits), on the GPU path."""
+    cfg = NOTEBOOKS[name]
+    cls = GPU_WignerDiracKvN4D if cfg["kvn"] else GPU_WignerDirac4D
+    f = make_frame(cls, cfg["params"], bound_p=7.0, FilterParticle=cfg["filter"])
+    n0 = _prepare_gpu(f, cfg)
+    g = GOLD[name]["init_norms"][0]
+    assert abs(n0.real - g) < 1e-11 * g
+
+
+@pytest.mark.parametrize("name", [pytest.param(n, marks=pytest.mark.xfail(
+    strict=True, reason="the notebook ran on another revision of the reference")) if n in OTHER_REVISION else n
+    for n in sorted(NOTEBOOKS)])
+def test_golden_notebook_run_norms_on_gpu(name):
+    """The trace norms the notebooks print during Run() (mask constant 7 for
+    p), first two iterations, on the GPU path; the four notebooks that ran
+    on another revision of the reference are expected to differ."""
+    cfg = NOTEBOOKS[name]
+    cls = GPU_WignerDiracKvN4D if cfg["kvn"] else GPU_WignerDirac4D
+    f = make_frame(cls, cfg["params"], bound_p=7.0, FilterParticle=cfg["filter"])
+    _prepare_gpu(f, cfg)
+    f.timeSteps = 1
     f.fileName = None
     f.Run()
-    for k in range(3):
-        assert abs(f.norms[k].real - g["run_norms"][k]) < 1e-10 * g["run_norms"][k], k
+    g = GOLD[name]["run_norms"]
+    for k in range(2):
+        assert abs(f.norms[k].real - g[k]) < 1e-9 * g[k], (k, f.norms[k], g[k])
 
 
 def _centred_dft2(X, fwd):
@@ -188,18 +225,16 @@ def _centred_dft2(X, fwd):
     return S * F
 
 
-@pytest.mark.parametrize("variant", ["tma", "cluster", "plain"])
+@pytest.mark.parametrize("variant", ["tma", "plain"])
 @pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-13), (np.complex64, 5e-6)])
 def test_dplane_r4_64(dtype, tol, variant, monkeypatch):
     """The 64^4 component-plane transforms of all four Dirac wrappers
-    (k_dplane_r4; for P <-> Theta k_dplane_r4t, k_dplane_r4c with
-    WIG_DPLANE_CLUSTER, or k_dplane_r4 with WIG_NO_DPLANE_TMA): against NumPy's 2-D FFT on sampled planes, and
+    (k_dplane_r4; for P <-> Theta k_dplane_r4t, or k_dplane_r4 with
+    WIG_NO_DPLANE_TMA): against NumPy's 2-D FFT on sampled planes, and
     against the generic plane kernels (k_dplane / k_dplane_g) on two whole
     components."""
     if variant == "plain":
         monkeypatch.setenv("WIG_NO_DPLANE_TMA", "1")
-    if variant == "cluster":
-        monkeypatch.setenv("WIG_DPLANE_CLUSTER", "1")
     p = small(64, fast=True)
     f = make_frame(GPU_WignerDirac4D, p, complex_dtype=dtype)
     tdt = torch.complex128 if dtype == np.complex128 else torch.complex64
@@ -292,3 +327,96 @@ def test_run_parity_a3_zero():
     for name in ["average_x", "energyKinetic", "energyPotential"]:
         assert rel_err(getattr(f, name), np.array([ob[name] for ob in obs])) < 1e-11, name
     assert err16(comps(f), o.W) < 1e-11
+
+
+def test_run_parity_nonseparable_field():
+    """A1 = exp(-(x-y)^2), A2 = 0.2/sqrt(1 + (x-y)^2): no low-rank form at the
+    Bopp-shifted points, so the plan holds A on every point (the reference
+    splices any expression into its kernel, GPU_WignerDirac4D.py:498-514)."""
+    p = small(16, False, True, potential_1_String="exp(-(x-y)*(x-y))",
+              potential_2_String="0.2/sqrt(1.0 + (x-y)*(x-y))")
+    f, o = pair(p, False, alias_w21=False, bound_p=15.0)
+    assert f._a_full
+    set_state(f, o, 11)
+    f.timeSteps = 3
+    f.fileName = None
+    f.Run()
+    Ws = o.pointers(False)
+    norms, obs = [], []
+    for _ in range(4):
+        n, ob = o.run_iteration(Ws, filter_particle=False, bound_p=15.0)
+        norms.append(n)
+        obs.append(ob)
+    assert rel_err(f.norms, np.array(norms)) < 1e-12
+    for name in ["average_x", "average_p_y", "energyKinetic", "energyPotential", "average_Alpha_1"]:
+        assert rel_err(getattr(f, name), np.array([ob[name] for ob in obs])) < 1e-11, name
+    assert err16(comps(f), o.W) < 1e-11
+
+
+def config5_params(seed=5000):
+    """Wigner-Dirac on 64^4: V = 0.3 (x^2 + y^2), symmetric-gauge field
+    A = (B/2)(-y, x, 0) with B ~ U[0.1, 0.5], D_lambda = 0.005, dt = 0.002,
+    delta = 1/N windows; returns (params, B, centre)."""
+    import math
+    rng = np.random.default_rng(seed)
+    B = float(rng.uniform(0.1, 0.5))
+    x0, y0 = (float(v) for v in rng.uniform(-2, 2, size=2))
+    n, amp_x, amp_p = 64, 8.0, 8.0
+    dx, dp = 2 * amp_x / n, 2 * amp_p / n
+    params = dict(gridDIM_p_y=n, gridDIM_y=n, gridDIM_p_x=n, gridDIM_x=n, dt=0.002,
+                  p_y_amplitude=amp_p, y_amplitude=amp_x, p_x_amplitude=amp_p, x_amplitude=amp_x,
+                  theta_y_amplitude=math.pi / dp, theta_x_amplitude=math.pi / dp,
+                  lambda_y_amplitude=math.pi / dx, lambda_x_amplitude=math.pi / dx,
+                  c=1.0, HBar=1.0, mass=1.0, potential_0_String="0.3*(x*x + y*y)",
+                  potential_1_String="-%r*y/2." % B, potential_2_String="%r*x/2." % B,
+                  potential_3_String="0.", D_1_potential_0_String="0.6*x", D_1_potential_1_String="0.",
+                  D_1_potential_2_String="%r/2." % B, D_theta_x=0.0, D_theta_y=0.0,
+                  D_lambda_x=0.005, D_lambda_y=0.005)
+    return params, B, (x0, y0)
+
+
+def test_config5_dirac_64_vs_oracle():
+    """The 64^4 symmetric-gauge configuration from a positive-energy spinor
+    (ParticleUp, theta -> p, x -> lambda, projector(+1), lambda -> x, the
+    FreeFiltered preparation), two Run() iterations with the fused loop,
+    against the oracle (about 18 GB of host memory and 3 minutes)."""
+    psutil = pytest.importorskip("psutil")
+    if psutil.virtual_memory().available < 32e9:
+        pytest.skip("the 64^4 Dirac oracle needs about 18 GB of host memory")
+    params, B, (x0, y0) = config5_params()
+    f, o = pair(params, False, alias_w21=False, bound_p=15.0)
+    Ws = all_w(f)
+    f.WignerDiracGaussian_ParticleUp_GPU(*Ws, 0.0, 0.0, x0, y0, 1.0, 1.0)
+    f.Fourier_Theta_To_P_64_64_4x4_GPU(*Ws)
+    f.Fourier_X_To_Lambda_64_64_4x4_GPU(*Ws)
+    f.ParticleProjector_GPU(*Ws, 1)
+    f.Fourier_Lambda_To_X_64_64_4x4_GPU(*Ws)
+    for k in (0, 5, 10, 15):
+        f.Real_GPU(Ws[k])
+    n0 = f.Normalize_4x4_GPU(*Ws)
+    o.particle_up(0.0, 0.0, x0, y0, 1.0, 1.0)
+    for W in o.W:
+        o.theta_to_p(W)
+    for W in o.W:
+        o.x_to_lambda(W)
+    o.projector(o.W, 1)
+    for W in o.W:
+        o.lambda_to_x(W)
+    for k in (0, 5, 10, 15):
+        o.real(o.W[k])
+    no = o.normalize(o.W)
+    assert abs(n0 - no) < 1e-12 * abs(no)
+    assert err16(comps(f), o.W) < 1e-12
+    f.timeSteps = 1
+    f.fileName = None
+    f.Run()
+    Wp = o.pointers(False)
+    norms, obs = [], []
+    for _ in range(2):
+        n, ob = o.run_iteration(Wp, filter_particle=False, bound_p=15.0)
+        norms.append(n)
+        obs.append(ob)
+    assert rel_err(f.norms, np.array(norms)) < 1e-12
+    for name in ["average_x", "average_y", "energyKinetic", "energyPotential"]:
+        assert rel_err(getattr(f, name), np.array([ob[name] for ob in obs])) < 1e-11, name
+    assert err16(comps(f), o.W) < 1e-10

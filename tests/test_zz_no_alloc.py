@@ -23,6 +23,7 @@ if not torch.cuda.is_available():
 
 from configs import cat_xp, config1, config2  # noqa: E402
 from frames import make_frame, rel_err  # noqa: E402
+from oracle.wigner4d import Wigner4DOracle  # noqa: E402
 from pywignercuda2_b200 import GPU_Wigner4D, _lib, expr  # noqa: E402
 from pywignercuda2_b200.device import stream_ptr  # noqa: E402
 
@@ -59,6 +60,17 @@ def test_noalloc_matches_plan_reduction_twice(dtype):
         assert _noalloc(f, f.W_init_gpu.tensor, cp, ep, ex, out) == 0
         got = out.cpu().numpy()
         assert rel_err(got, want) < tol, (got, want)
+        # and the oracle's norm and raw observables of the same (rounded) state
+        o = Wigner4DOracle(params)
+        Wh = W0.astype(dtype).astype(np.complex128)
+        n = o.norm(Wh)
+        assert abs(complex(got[0], got[1]) - n) < 1e-12 * abs(n)
+        ob = o.observables(Wh)
+        raw = got[_lib.WIG4D_NOBS:]
+        names = ["average_x", "average_p_x", "average_x_square", "average_p_x_square", "average_y",
+                 "average_p_y", "average_y_square", "average_p_y_square", "energy"]
+        for k, name in enumerate(names):
+            assert abs(raw[2 + k] - ob[name]) <= 1e-11 * max(abs(ob[name]), abs(n)), name
 
 
 def test_noalloc_rejects_grids_above_the_limit():
