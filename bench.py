@@ -201,10 +201,14 @@ def bench_batched(steps):
     cfg = replicas.shard(config4(0), rank, ws)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     frames = []
+    tuned = {}
     for params, c in cfg:
-        f = make_frame(GPU_Wigner4D, dict(params, timeSteps=steps - 1), complex_dtype=np.complex64)
+        f = make_frame(GPU_Wigner4D, dict(params, timeSteps=steps - 1), complex_dtype=np.complex64,
+                       autotune=True)
         f.W_init_gpu.set(gaussian_xp(f._coords, c).astype(np.complex64))
         frames.append(f)
+        if f.autotune_choice["timed"]:
+            tuned["%d^4" % f.shape[0]] = f.autotune_choice
     pts_rank = sum(int(np.prod(f.shape)) for f in frames)
     pts = int(replicas.sum_over_ranks(pts_rank))
     batch = WignerBatch(frames)
@@ -221,7 +225,7 @@ def bench_batched(steps):
     del batch, frames, hists
     ms_plain = 0.0
     for params, c in cfg:
-        f = make_frame(GPU_Wigner4D, dict(params, timeSteps=steps - 1))
+        f = make_frame(GPU_Wigner4D, dict(params, timeSteps=steps - 1), autotune=True)
         f.W_init_gpu.set(gaussian_xp(f._coords, c))
         h = torch.empty((steps, 11), dtype=torch.float64, device="cuda")
         f.run_device(f.W_init_gpu, 3, h)
@@ -239,7 +243,8 @@ def bench_batched(steps):
             "scaling": "strong", "parallelism": "instances split over ranks" if ws > 1 else "single",
             "gp_steps_per_s": pts * steps / (ms_batch / 1e3), "ms": ms_batch, "finite": finite,
             "one_at_a_time_plain_c128": {"gp_steps_per_s": pts * steps / (ms_plain / 1e3), "ms": ms_plain},
-            "speedup_vs_one_at_a_time_plain": ms_plain / ms_batch}
+            "speedup_vs_one_at_a_time_plain": ms_plain / ms_batch,
+            "autotune": tuned}
 
 
 def _dirac_frame(steps, complex_dtype=np.complex128):
@@ -373,6 +378,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--no-dirac", action="store_true", help="skip the Wigner-Dirac line")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the 1000-step accuracy block")
+    ap.add_argument("--profile-form", choices=["c128", "c64", "tc", "tc-general"],
+                    help="only run two Run() iterations of one 64^4 form (a small case for ncu) and exit")
     ap.add_argument("--dirac-steps", type=int, default=20)
     ap.add_argument("--dirac-passes", choices=["c128", "c64"],
                     help="only time each pass of one Wigner-Dirac iteration in this dtype and exit")
@@ -380,6 +387,25 @@ def main():
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_form:
+        kw = {"c128": {}, "c64": {"complex_dtype": np.complex64},
+              "tc": {"complex_dtype": np.complex64, "tensor_cores": True},
+              "tc-general": {"complex_dtype": np.complex64, "tensor_cores": True}}[args.profile_form]
+        from configs import config2
+        from frames import make_frame
+        from pywignercuda2_b200 import GPU_Wigner4D
+        params, c = config2(seed=0, n=64)
+        if args.profile_form == "tc-general":     # the notebooks' windows, delta N = 0.716
+            params.update(theta_x_amplitude=9.0, theta_y_amplitude=9.0, lambda_x_amplitude=9.0,
+                          lambda_y_amplitude=9.0)
+        f = make_frame(GPU_Wigner4D, params, complex_dtype=kw.pop("complex_dtype", np.complex128), **kw)
+        f.CatState_GPU(f.W_init_gpu, c[0], c[1], c[2], c[3], 1.5, 0.0)
+        f.timeSteps = 1
+        f.fileName = None
+        f.Run()
+        print(json.dumps({"profile_form": args.profile_form, "kernels": f.plan_info(),
+                          "energy": [float(e) for e in f.energy]}), flush=True)
+        return 0
     if args.dirac_passes:
         from pywignercuda2_b200.dirac4d import NAMES
         f, _, (x0, y0) = _dirac_frame(2, np.complex64 if args.dirac_passes == "c64" else np.complex128)
@@ -526,7 +552,9 @@ def main():
                                 else "fallback",
                                 "issued_tensor_flops_per_launch": tc_flops,
                                 "dense_dft_flops_per_launch": dft_flops,
-                                "hbm_frac": state_bytes / (dtc / 1e3) / 1e9 / peak},
+                                "hbm_frac": state_bytes / (dtc / 1e3) / 1e9 / peak,
+                                "traffic": _traffic().get(("k_tc64<pot>" if ptc >= ktc else "k_tc64<kin>",
+                                                           "64x64x64x64_c64"))},
                    "error_vs_c128": dict(_hist_err(htc, h128), steps=Wm + K)}
     del ftc
 

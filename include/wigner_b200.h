@@ -141,7 +141,8 @@ typedef struct {
        vectors; FP64 sums above the row level), for any delta.  1 needs
        WIG_C64 on a 64^4 grid, factor tables that do not span both in-plane
        axes of a half-step, positive deltas and the same |delta| on the two
-       in-plane axes of each half-step (else WIG_ERR_UNSUPPORTED).        */
+       in-plane axes of each half-step (else WIG_ERR_UNSUPPORTED).  2 sets
+       k_tc64 up as a candidate of wig4d_autotune and starts with 0.       */
     int transform;
 } wig4d_desc;
 
@@ -264,6 +265,25 @@ int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
    wig4d_desc.transform = 1). */
 int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
 
+
+/*
+ * The project's autotuner (no counterpart in the reference): times the
+ * kernel choices this plan has on a scratch copy of a Gaussian state
+ * (`iterations` Run() iterations each, CUDA events on `stream`) and keeps
+ * the fastest.  The candidates are the 64^4 engines (k_r4 with cluster or
+ * plain stores, complex128 k_r4t, and k_tc64 when the plan was made with
+ * wig4d_desc.transform = 2) or, for the other kernels, k_kin48 against
+ * k_kinetic on 48 x 48 planes and the columns per CTA of k_potential_g
+ * (8, 4, 2, or k_potential).  The choice is cached per (shape, dtype,
+ * kernel path) for the process: later plans with the same key take it
+ * without timing unless flags has WIG_TUNE_FORCE.  choice_out (host, 4
+ * ints, may be NULL) receives the engine (0 k_r4 plain, 1 k_r4 cluster,
+ * 2 k_r4t, 3 k_tc64, 4 the per-size kernels), k_kin48 (1/0), the columns
+ * per CTA and the number of candidates timed.  Allocates a scratch state;
+ * synchronous; call it outside any stream capture.
+ */
+#define WIG_TUNE_FORCE 1
+int wig4d_autotune(wig4d_plan* plan, int iterations, int flags, void* stream, int* choice_out);
 
 /* Bytes of device memory the plan holds (tables, partial sums). */
 long long wig4d_plan_device_bytes(const wig4d_plan* plan);

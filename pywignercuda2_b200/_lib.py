@@ -105,6 +105,7 @@ SIGNATURES = {
     "wig4d_init_gaussian": [_P, _P, _D, _D, _D, _D, _D, _D, _D, _D, _P],
     "wig4d_init_cat_xtheta": [_P, _P, _D, _D, _D, _D, _D, _D, _D, _D, _P],
     "wig4d_plan_device_bytes": [_P],
+    "wig4d_autotune": [_P, _I, _I, _P, _IP],
     "wig4d_observables_noalloc": [_P, _IP, _I, _P, _P, _P, _P, _P, _P, _D, _D, _P, _P],
     "wigd_plan_create": [ctypes.POINTER(DescDirac), ctypes.POINTER(_P)],
     "wigd_plan_destroy": [_P],

@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <type_traits>
 #include <vector>
@@ -743,6 +744,11 @@ struct wig4d_plan {
     bool r4;                       // 64^4 Run(): k_r4 (16 points per thread) on its LA / LB layouts
     bool r4t;                      // complex128 64^4 Run(): k_r4 with TMA plane loads (k_r4t)
     bool r4_cluster;               // k_r4 launched as clusters with full-sector stores
+    bool kin48;                    // 48 x 48 kinetic planes: k_kin48 (else k_kinetic)
+    int pot_gmax;                  // k_potential_g: at most this many columns per CTA (< 2: k_potential)
+    bool tc_ready;                 // k_tc64's buffers exist (wig4d_desc.transform 1 or 2)
+    int tuned;                     // wig4d_autotune has set the choices above
+    bool r4t_ready;                // k_r4t's tensor map and attributes are set
     int dense_n;                   // > 0: general-delta half-steps fused (k_dense_half, N^4 grids)
     const void* dmat[4];           // FAFT matrices per axis (|delta|), when dense_n > 0
     void* tw64;                    // k_r4 twiddle table (64 complex of the plan's dtype)
@@ -812,7 +818,7 @@ static int launch_kinetic(wig4d_plan* p, C* W, const double* d_norm, cudaStream_
     const int npy = p->shape[0], npx = p->shape[2];
     const unsigned grid = (unsigned)(npy * npx);
     const double2 sc = make_double2(p->kin_scale, 0.0);
-    if (NY == 48 && NX == 48 && !getenv("WIG_NO_K48")) {   // 48 x 48 planes in registers
+    if (NY == 48 && NX == 48 && p->kin48) {                 // 48 x 48 planes in registers
         const size_t sm = k48::smem_bytes<C>();
         WIG_CUDA(cudaFuncSetAttribute(k_kin48<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         k_kin48<C><<<grid, k48::NT, sm, st>>>(W, npy, npx, kin_set<C>(p), sc, d_norm);
@@ -843,7 +849,7 @@ static bool launch_potential_gn(wig4d_plan* p, C* W, double* partials, cudaStrea
         return false;
     } else {
         typedef PotCfg<C, NPY, NPX, G> P;
-        if (P::bytes() > 227 * 1024 || p->shape[3] % G != 0)
+        if (G > p->pot_gmax || P::bytes() > 227 * 1024 || p->shape[3] % G != 0)
             return launch_potential_gn<C, NPY, NPX, G / 2>(p, W, partials, st, sc);
         auto kern = k_potential_g<C, NPY, NPX, G>;
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::bytes()) != cudaSuccess)
@@ -855,7 +861,7 @@ static bool launch_potential_gn(wig4d_plan* p, C* W, double* partials, cudaStrea
 }
 template <class C, int NPY, int NPX>
 static bool launch_potential_g(wig4d_plan* p, C* W, double* partials, cudaStream_t st, double2 sc) {
-    if (getenv("WIG_NO_POT_G")) return false;
+    if (p->pot_gmax < 2) return false;
     constexpr int G0 = sizeof(C) == 16 ? 4 : (NPY * NPX <= 48 * 48 ? 4 : 8);
     return launch_potential_gn<C, NPY, NPX, G0>(p, W, partials, st, sc);
 }
@@ -1042,10 +1048,23 @@ static int ensure_w_maps(wig4d_plan* p, const void* W) {
     return WIG_OK;
 }
 
+// k_r4 with TMA plane loads (complex128): the LA map of the ping-pong buffer
+// (the LB map of the caller's state is made at the first run).
+static int ensure_r4t(wig4d_plan* p) {
+    if (p->r4t_ready) return WIG_OK;
+    int r;
+    if ((r = encode_plane_map(&p->map_t_load, p->pingpong))) return r;
+    WIG_CUDA(cudaFuncSetAttribute(k_r4t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4t_smem_bytes()));
+    WIG_CUDA(cudaFuncSetAttribute(k_r4t<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4t_smem_bytes()));
+    p->r4t_ready = true;
+    return WIG_OK;
+}
+
 extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
     if (!desc || !out) return WIG_ERR_INVALID_ARG;
     *out = nullptr;
     if (desc->dtype != WIG_C128 && desc->dtype != WIG_C64) return WIG_ERR_INVALID_ARG;
+    if (desc->transform < 0 || desc->transform > 2) return WIG_ERR_INVALID_ARG;
     for (int a = 0; a < 4; ++a) {
         if (desc->shape[a] < 2 || desc->shape[a] > 1024 || (desc->shape[a] & 1)) return WIG_ERR_UNSUPPORTED;
         if (!desc->coord[a]) return WIG_ERR_INVALID_ARG;
@@ -1063,6 +1082,10 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
     p->npts = (long long)p->shape[0] * p->shape[1] * p->shape[2] * p->shape[3];
     p->dv_norm = desc->dv_norm;
     p->dv_obs = desc->dv_obs;
+    // kernel choices (wig4d_autotune may change them; the variables override
+    // the defaults for comparisons in tests)
+    p->kin48 = getenv("WIG_NO_K48") == nullptr;
+    p->pot_gmax = getenv("WIG_NO_POT_G") ? 1 : 8;
     // total scalar of a fused half-step: (2 N d)^2 per transformed axis (the
     // forward and the inverse FAFT) times the wrapper divisors.
     p->kin_scale = desc->kin_post_scale;
@@ -1234,13 +1257,9 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
         const char* kern = getenv("WIG_FAST64_KERNEL");
         p->r4 = true;
         if (desc->dtype == WIG_C128 && kern && strcmp(kern, "r4t") == 0) {
-            // k_r4 with TMA plane loads: LA map of the ping-pong buffer now,
-            // LB map of the caller's state at the first run
             int r;
-            if ((r = encode_plane_map(&p->map_t_load, p->pingpong))) { free_plan(p); return r; }
+            if ((r = ensure_r4t(p))) { free_plan(p); return r; }
             p->r4t = true;
-            cudaFuncSetAttribute(k_r4t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4t_smem_bytes());
-            cudaFuncSetAttribute(k_r4t<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4t_smem_bytes());
         }
         p->r4_cluster = !(kern && strcmp(kern, "r4") == 0);
         if (cudaMalloc(&p->tw64, 64 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
@@ -1262,7 +1281,7 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
     }
     // tensor-core transforms (k_tc64): complex64 64^4, separable factors,
     // positive deltas, the same |delta| on both in-plane axes of each half-step
-    if (desc->transform == 1) {
+    if (desc->transform == 1 || desc->transform == 2) {
         const bool ok64 = desc->dtype == WIG_C64 && p->shape[0] == 64 && p->shape[1] == 64 && p->shape[2] == 64 &&
                           p->shape[3] == 64;
         bool ok = ok64 && separable(desc->kin, desc->n_kin, 1, 3) && separable(desc->pot, desc->n_pot, 0, 2);
@@ -1313,7 +1332,8 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             cudaFuncSetAttribute(k_tc64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc64::SMEM) != cudaSuccess) {
             wig_set_cuda_error(cudaGetLastError(), "k_tc64 attributes"); free_plan(p); return WIG_ERR_CUDA;
         }
-        p->tc = true;
+        p->tc = desc->transform == 1;
+        p->tc_ready = true;
     }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { wig_set_cuda_error(e, "wig4d_plan_create"); free_plan(p); return WIG_ERR_CUDA; }
@@ -1790,6 +1810,143 @@ extern "C" int wig4d_run_ex(wig4d_plan* p, void* W, int iterations, double* d_hi
 
 extern "C" int wig4d_run(wig4d_plan* p, void* W, int iterations, double* d_history, void* stream) {
     return wig4d_run_ex(p, W, iterations, d_history, 0, stream);
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: the kernel choices of a plan, timed on a scratch state.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct TuneKey {
+    int shape[4], dtype, fast64, dense_n, tc_ready;
+    bool operator<(const TuneKey& o) const { return memcmp(this, &o, sizeof(*this)) < 0; }
+};
+struct TuneChoice { int engine, kin48, pot_gmax; };
+
+// engine: 0 k_r4 plain stores, 1 k_r4 cluster stores, 2 k_r4t, 3 k_tc64,
+// 4 the CUDA-core path of a plan without the 64^4 radix kernels
+int apply_choice(wig4d_plan* p, const TuneChoice& c) {
+    if (c.engine == 2) {
+        const int r = ensure_r4t(p);
+        if (r) return r;
+    }
+    p->tc = c.engine == 3;
+    p->r4_cluster = c.engine == 1;
+    p->r4t = c.engine == 2;
+    p->kin48 = c.kin48 != 0;
+    p->pot_gmax = c.pot_gmax;
+    if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
+    return WIG_OK;
+}
+
+TuneChoice current_choice(const wig4d_plan* p) {
+    TuneChoice c;
+    c.engine = p->tc ? 3 : (p->r4 ? (p->r4t ? 2 : (p->r4_cluster ? 1 : 0)) : 4);
+    c.kin48 = p->kin48;
+    c.pot_gmax = p->pot_gmax;
+    return c;
+}
+
+std::mutex tune_mu;
+std::map<TuneKey, TuneChoice> tune_cache;
+
+}  // namespace
+
+extern "C" int wig4d_autotune(wig4d_plan* p, int iterations, int flags, void* stream, int* choice_out) {
+    if (!p || iterations < 1 || (flags & ~WIG_TUNE_FORCE)) return WIG_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    TuneKey key;
+    memset(&key, 0, sizeof(key));
+    memcpy(key.shape, p->shape, sizeof(key.shape));
+    key.dtype = p->dtype; key.fast64 = p->fast64; key.dense_n = p->dense_n; key.tc_ready = p->tc_ready;
+    {
+        std::lock_guard<std::mutex> lk(tune_mu);
+        auto it = tune_cache.find(key);
+        if (it != tune_cache.end() && !(flags & WIG_TUNE_FORCE)) {
+            const int r = apply_choice(p, it->second);
+            if (r) return r;
+            p->tuned = 1;
+            if (choice_out) { choice_out[0] = it->second.engine; choice_out[1] = it->second.kin48;
+                              choice_out[2] = it->second.pot_gmax; choice_out[3] = 0; }
+            return WIG_OK;
+        }
+    }
+    // candidates: the 64^4 engines, then (for the generic kernels) the 48 x 48
+    // kinetic kernel and the potential kernel's columns per CTA
+    std::vector<TuneChoice> engines;
+    const TuneChoice base = current_choice(p);
+    if (p->r4) {
+        engines.push_back({1, base.kin48, base.pot_gmax});
+        engines.push_back({0, base.kin48, base.pot_gmax});
+        if (p->dtype == WIG_C128) engines.push_back({2, base.kin48, base.pot_gmax});
+    } else {
+        engines.push_back({4, base.kin48, base.pot_gmax});
+    }
+    if (p->tc_ready) engines.push_back({3, base.kin48, base.pot_gmax});
+    const size_t esz = p->dtype == WIG_C128 ? 16 : 8;
+    void* scratch = nullptr;
+    double* hist = nullptr;
+    if (cudaMalloc(&scratch, (size_t)p->npts * esz) != cudaSuccess) return WIG_ERR_ALLOC;
+    if (cudaMalloc(&hist, (size_t)(iterations + 2) * WIG4D_NOBS * sizeof(double)) != cudaSuccess) {
+        cudaFree(scratch); return WIG_ERR_ALLOC;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const TuneChoice saved = base;
+    int status = WIG_OK;
+    float tried = 0;
+    auto time_choice = [&](const TuneChoice& c, float* ms) -> int {
+        int s = apply_choice(p, c);
+        if (s) return s;
+        s = wig4d_init_gaussian(p, scratch, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0, 1.0, stream);
+        if (s) return s;
+        if ((s = wig4d_run(p, scratch, 2, hist, stream))) return s;   // warm-up: attributes, graph
+        WIG_CUDA(cudaEventRecord(e0, st));
+        if ((s = wig4d_run(p, scratch, iterations, hist, stream))) return s;
+        WIG_CUDA(cudaEventRecord(e1, st));
+        WIG_CUDA(cudaEventSynchronize(e1));
+        WIG_CUDA(cudaEventElapsedTime(ms, e0, e1));
+        tried += 1;
+        return WIG_OK;
+    };
+    TuneChoice best = base;
+    float best_ms = 3.4e38f;
+    for (const TuneChoice& c : engines) {
+        float ms;
+        if ((status = time_choice(c, &ms))) break;
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    if (!status && best.engine == 4) {
+        // generic kernels: the 48 x 48 kinetic kernel, then the potential's G
+        if (p->shape[1] == 48 && p->shape[3] == 48) {
+            TuneChoice c = best;
+            c.kin48 = !best.kin48;
+            float ms;
+            if (!(status = time_choice(c, &ms)) && ms < best_ms) { best_ms = ms; best = c; }
+        }
+        for (int g : {8, 4, 2, 1}) {
+            if (status || g == best.pot_gmax) continue;
+            TuneChoice c = best;
+            c.pot_gmax = g;
+            float ms;
+            if (!(status = time_choice(c, &ms)) && ms < best_ms) { best_ms = ms; best = c; }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(hist);
+    cudaFree(scratch);
+    if (status) { apply_choice(p, saved); return status; }
+    if ((status = apply_choice(p, best))) return status;
+    p->tuned = 1;
+    {
+        std::lock_guard<std::mutex> lk(tune_mu);
+        tune_cache[key] = best;
+    }
+    if (choice_out) { choice_out[0] = best.engine; choice_out[1] = best.kin48; choice_out[2] = best.pot_gmax;
+                      choice_out[3] = (int)tried; }
+    return WIG_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -20,7 +20,11 @@ Extra attributes a frame may set (defaults reproduce the reference):
   built in float64 and rounded once, float64 reductions).
 * ``tensor_cores``: True (complex64 64^4 grids, any delta) runs Run()'s
   64-point transforms as dense FAFT GEMMs on the tensor cores (fp16 hi + lo
-  operands, FP32 accumulation; k_tc64) instead of the CUDA-core kernels.
+  operands, FP32 accumulation; k_tc64) instead of the CUDA-core kernels;
+  "auto" makes them a candidate of the autotuner.
+* ``autotune``: True times the plan's kernel choices once per (grid, dtype,
+  kernel path) in the process (wig4d_autotune) and keeps the fastest; the
+  choice is in ``self.autotune_choice``.  "force" times it again.
 * ``round_constants``: True reproduces the reference's '%f' formatting of the
   device constants (GPU_Wigner4D.py:128-150); False uses full precision.
 * ``snapshotEvery``: K > 0 makes Run() keep the normalised state every K
@@ -53,6 +57,7 @@ class GPU_Wigner4D:
     complex_dtype = np.complex128
     round_constants = True
     tensor_cores = False
+    autotune = False
 
     def __init__(self):
         require_cuda()
@@ -173,9 +178,17 @@ class GPU_Wigner4D:
         d.dv_norm = self.dx * self.dp_x * self.dy * self.dp_y
         d.dv_obs = self._c("dx") * self._c("dy") * self._c("dp_x") * self._c("dp_y")
         plan = ctypes.c_void_p()
-        d.transform = 1 if self.tensor_cores else 0
+        d.transform = 2 if self.tensor_cores == "auto" else (1 if self.tensor_cores else 0)
         _lib.call("wig4d_plan_create", ctypes.byref(d), ctypes.byref(plan))
         self._plan = plan
+        self.autotune_choice = None
+        if self.autotune:
+            ch = (ctypes.c_int * 4)()
+            _lib.call("wig4d_autotune", plan, 3, 1 if self.autotune == "force" else 0, stream_ptr(), ch)
+            engines = {0: "k_r4 plain stores", 1: "k_r4 cluster stores", 2: "k_r4t", 3: "k_tc64",
+                       4: "per-size kernels"}
+            self.autotune_choice = {"engine": engines[ch[0]], "k_kin48": bool(ch[1]), "pot_columns": ch[2],
+                                    "timed": ch[3]}
         self._desc = d
         self._obs_buf = torch.empty(2 * _lib.WIG4D_NOBS, dtype=torch.float64, device="cuda")
 

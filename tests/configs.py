@@ -12,14 +12,19 @@ import numpy as np
 
 
 def w4d_params(n, amp=8.0, q=0.1, kappa=0.05, D=0.01, dt=0.01, n_p=None):
+    """delta = 1/N on every axis.  The reference steps theta with the x grid
+    size and lambda with the p grid size (dtheta = 2 theta_amp / N_x,
+    dlambda = 2 lambda_amp / N_p, GPU_Wigner4D.py:95-98), so on an N_x x N_p
+    grid delta_p = dp dtheta / 2 pi = 1/N_p needs theta_amp = pi N_x / (N_p dp)
+    and delta_x = 1/N_x needs lambda_amp = pi N_p / (N_x dx)."""
     n_p = n if n_p is None else n_p
     dx = 2 * amp / n
     dp = 2 * amp / n_p
     return dict(
         gridDIM_p_y=n_p, gridDIM_y=n, gridDIM_p_x=n_p, gridDIM_x=n,
         p_y_amplitude=amp, y_amplitude=amp, p_x_amplitude=amp, x_amplitude=amp,
-        theta_y_amplitude=math.pi / dp, theta_x_amplitude=math.pi / dp,
-        lambda_y_amplitude=math.pi / dx, lambda_x_amplitude=math.pi / dx,
+        theta_y_amplitude=math.pi * n / (n_p * dp), theta_x_amplitude=math.pi * n / (n_p * dp),
+        lambda_y_amplitude=math.pi * n_p / (n * dx), lambda_x_amplitude=math.pi * n_p / (n * dx),
         dt=dt, mass=1.0, timeSteps=0,
         kineticString="0.5*(p_x*p_x + p_y*p_y)",
         potentialString="0.5*(x*x + y*y) + %r*(pow(x,4) + pow(y,4)) + %r*x*y" % (q, kappa),

@@ -61,3 +61,32 @@ def test_batch_unequal_steps_rejected():
     fr[1][0].timeSteps = 3
     with pytest.raises(ValueError):
         WignerBatch([f for f, _ in fr]).Run()
+
+
+def test_autotune_choices_and_cache():
+    """wig4d_autotune: the tuned plan gives the untuned plan's results, the
+    choice is reported, and a second plan with the same key takes the cached
+    choice without timing."""
+    from configs import config1, config2, cat_xp
+    from frames import rel_err
+    out = {}
+    for n, dtype, tc in ((48, np.complex128, False), (64, np.complex64, "auto")):
+        p, c = (config1(2, n) if n == 48 else config2(2, n))
+        ref = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
+        f = make_frame(GPU_Wigner4D, p, complex_dtype=dtype, autotune="force", tensor_cores=tc)
+        ch = f.autotune_choice
+        assert ch is not None and ch["timed"] >= 1
+        g = make_frame(GPU_Wigner4D, p, complex_dtype=dtype, autotune=True, tensor_cores=tc)
+        assert g.autotune_choice["timed"] == 0 and g.autotune_choice["engine"] == ch["engine"]
+        W0 = cat_xp(f._coords, c).astype(dtype)
+        for fr in (ref, f):
+            fr.W_init_gpu.set(W0)
+            fr.timeSteps = 4
+            fr.fileName = None
+            fr.Run()
+        tol = 1e-12 if dtype == np.complex128 else 3e-4
+        assert rel_err(f.energy, ref.energy) < tol
+        assert rel_err(f.W_init_gpu.get(), ref.W_init_gpu.get()) < (1e-10 if dtype == np.complex128 else 1e-4)
+        out[n] = ch
+    assert out[64]["engine"] in ("k_r4 plain stores", "k_r4 cluster stores", "k_tc64")
+    assert out[48]["engine"] == "per-size kernels"

@@ -447,6 +447,8 @@ def test_run_config3_grid_vs_oracle():
     o = Wigner4DOracle(p)
     W0 = o.ho_ground(0.4, -0.3, 0.2, -0.1, 1.0, 1.0, 1.0)
     Wo, obs = o.run(W0, 2)
+    # delta = 1/N on every axis, so the energy of the ground state moves slowly
+    assert np.all(np.abs(np.diff(obs["energy"])) < 0.01 * abs(obs["energy"][0]))
     for dtype, tol in ((np.complex128, 1e-12), (np.complex64, 5e-5)):
         f = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
         assert f.shape == (128, 64, 128, 64)
