@@ -123,7 +123,8 @@ def accuracy_1000(steps=1000):
     drop-in from the same initial state (the drop-in matches the FP64 oracle
     to 1e-12 over 20 iterations at 64^4 and 3 iterations on config 3's grid,
     tests/test_gpu_tc.py and tests/test_gpu_w4d.py): the radix complex64
-    kernels and the tensor-core kernels at 64^4 (config 2), and the complex64
+    kernels, the tensor-core kernels and complex64 storage with FP64
+    transforms at 64^4 (config 2), and the complex64
     form on config 3's 64 x 128 x 64 x 128 grid."""
     import torch
     from configs import w4d_params
@@ -140,7 +141,8 @@ def accuracy_1000(steps=1000):
     f, W0 = _frame(np.complex128)
     h128, w128 = run(f, W0)
     del f
-    for name, kw in (("c64_radix", {}), ("c64_tensor_cores", {"tensor_cores": True})):
+    for name, kw in (("c64_radix", {}), ("c64_tensor_cores", {"tensor_cores": True}),
+                     ("c64_storage_fp64_transforms", {"fp64_transforms": True})):
         g, _ = _frame(np.complex64, **kw)
         h, w = run(g, W0)
         e = _hist_err(h, h128)
@@ -521,6 +523,29 @@ def main():
                                                         "64x64x64x64_c64"))}
     del f32
 
+    # ---- mixed form: complex64 state in memory, FP64 transforms and factors ----
+    fmx, _ = _frame(np.complex64, fp64_transforms=True)
+    fmx.W_init_gpu.set(W0.astype(np.complex64))
+    histmx = torch.empty_like(hist)
+    fmx.run_device(fmx.W_init_gpu, Wm, histmx)
+    torch.cuda.synchronize()
+    e0.record(st)
+    fmx.run_device(fmx.W_init_gpu, K, histmx)
+    e1.record(st)
+    torch.cuda.synchronize()
+    msmx = e0.elapsed_time(e1)
+    hmx = histmx[:K].cpu().numpy()
+    kmx, pmx, _ = [m / K for m in fmx.run_device_timed(fmx.W_init_gpu, K, histmx)]
+    dmx = max(kmx, pmx)
+    mixed_form = {"dtype": "c64 state, FP64 transforms and factors", "kernel": "k_r4<double2, ., ., float2>",
+                  "steps_per_s": K / (msmx / 1e3), "speedup_vs_plain": (K / (msmx / 1e3)) / (K / (ms / 1e3)),
+                  "kinetic_ms": kmx, "potential_ms": pmx,
+                  "roofline": {"bound": "hbm", "achieved": state_bytes / (dmx / 1e3) / 1e9, "peak": peak,
+                               "unit": "GB/s", "frac": state_bytes / (dmx / 1e3) / 1e9 / peak,
+                               "algorithmic_bytes_per_launch": state_bytes},
+                  "error_vs_c128": dict(_hist_err(hmx, h128), steps=Wm + K)}
+    del fmx
+
     # ---- tensor-core form (k_tc64: the 64-point transforms as dense GEMMs on
     # tcgen05, split fp16, FP32 accumulation) on the same workload ---------------
     ftc, _ = _frame(np.complex64, tensor_cores=True)
@@ -586,6 +611,7 @@ def main():
             "grid_point_steps_per_s": value * P,
             "precision_form": precision,
             "tensor_core_form": tensor_form,
+            "mixed_form": mixed_form,
             "gpu_launches": (4 * K + 4) if run64 in ("r4", "r4t") else (3 * K + 3),
             "finite": finite, "roofline": roofline, "clocks": clocks,
             "e2e": {"value": ws * K / (e2e_ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d / K,
@@ -599,6 +625,7 @@ def main():
     line["metric_ratio"] = {
         "tensor_core_vs_plain": tensor_form["speedup_vs_plain"],
         "fp32_radix_vs_plain": precision["speedup_vs_plain"],
+        "c64_storage_fp64_transforms_vs_plain": mixed_form["speedup_vs_plain"],
         "batched_fp32_vs_one_at_a_time_plain": line.get("batched_form", {}).get("speedup_vs_one_at_a_time_plain"),
         "note": "steps/s ratios at 64^4 on the same GPU and step count; errors after 1000 steps are in "
                 "accuracy_1000_steps (target <= 1e-6 in norm and energy)"}

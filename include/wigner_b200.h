@@ -142,7 +142,10 @@ typedef struct {
        WIG_C64 on a 64^4 grid, factor tables that do not span both in-plane
        axes of a half-step, positive deltas and the same |delta| on the two
        in-plane axes of each half-step (else WIG_ERR_UNSUPPORTED).  2 sets
-       k_tc64 up as a candidate of wig4d_autotune and starts with 0.       */
+       k_tc64 up as a candidate of wig4d_autotune and starts with 0.  3 (a
+       WIG_C64 plan on the 64^4 radix path) keeps the complex64 state in
+       memory but runs the transforms and factors in FP64 (k_r4 with
+       complex128 arithmetic on complex64 storage).                       */
     int transform;
 } wig4d_desc;
 
@@ -262,7 +265,8 @@ int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
    radix Run() kernels (1 or 0 each); info[3] the 64^4 Run() kernels: 0 none,
    3 k_r4 (16 points per thread, the default), 4 k_r4t (complex128 k_r4 with
    TMA plane loads, WIG_FAST64_KERNEL=r4t), 6 k_tc64 (tensor-core transforms,
-   wig4d_desc.transform = 1). */
+   wig4d_desc.transform = 1), 7 k_r4 with FP64 transforms on complex64
+   storage (wig4d_desc.transform = 3). */
 int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
 
 

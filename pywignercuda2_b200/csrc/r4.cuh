@@ -123,6 +123,17 @@ __device__ __forceinline__ void st_sector(float2* p, const float2 (&v)[4]) {
                  : "memory");
 }
 
+// storage <-> arithmetic types (the mixed form: complex64 in memory, FP64
+// transforms)
+template <class C> __device__ __forceinline__ C widen(double2 v) { return v; }
+template <class C> __device__ __forceinline__ C widen(float2 v);
+template <> __device__ __forceinline__ double2 widen<double2>(float2 v) { return make_double2(v.x, v.y); }
+template <> __device__ __forceinline__ float2 widen<float2>(float2 v) { return v; }
+template <class S> __device__ __forceinline__ S narrow(double2 v);
+template <> __device__ __forceinline__ double2 narrow<double2>(double2 v) { return v; }
+template <> __device__ __forceinline__ float2 narrow<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+template <class S> __device__ __forceinline__ S narrow(float2 v) { return v; }
+
 template <class C> __device__ __forceinline__ void make_tw(C* tw);
 template <> __device__ __forceinline__ void make_tw<double2>(double2* tw) { make_twiddles(tw, 64); }
 template <> __device__ __forceinline__ void make_tw<float2>(float2* tw) { ff::make_norm_twiddles(tw); }
@@ -140,12 +151,14 @@ constexpr size_t r4_smem_bytes() { return sizeof(C) * (64 * 64 + 64) + sizeof(do
 // CL: launched as clusters of the IL planes f1 = IL m .. IL m + IL - 1 that
 // share each destination sector; the stores then go through distributed
 // shared memory so that every 32-byte sector is written whole (see the end).
-template <class C, bool KIN, bool CL>
+// S: the state's type in memory (C by default); S = float2 with C = double2
+// is the mixed form, complex64 storage with FP64 transforms and factors.
+template <class C, bool KIN, bool CL, class S = C>
 __global__ void __launch_bounds__(r4::NT, (sizeof(C) == 16 ? 2 : 4))
-k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__ PV, const C* __restrict__ gtw,
+k_r4(const S* __restrict__ src, S* __restrict__ dst, const double2* __restrict__ PV, const C* __restrict__ gtw,
      double2 scale, const double* __restrict__ d_norm, ObsTabs ob, double* __restrict__ partials) {
     using namespace r4;
-    constexpr int IL = Il<C>::v, NQ = 64 / IL;
+    constexpr int IL = Il<S>::v, NQ = 64 / IL;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* s = reinterpret_cast<C*>(smraw);
     C* tw = s + 64 * 64;
@@ -154,12 +167,12 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
     const int ac = t & 15, ar = t >> 4;
     C v[16];
     {
-        const C* g = src + ((((long long)ar * NQ + ac / IL) * 64 + f0) * 64 + f1) * IL + (ac % IL);
+        const S* g = src + ((((long long)ar * NQ + ac / IL) * 64 + f0) * 64 + f1) * IL + (ac % IL);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                v[4 * i + j] = g[(long long)i * (16LL * 64 * 64 * 64) + (long long)j * (16LL * 64 * 64)];
+                v[4 * i + j] = widen<C>(g[(long long)i * (16LL * 64 * 64 * 64) + (long long)j * (16LL * 64 * 64)]);
     }
     if (t < 64) tw[t] = gtw[t];
     if (t < 128) pvs[t] = __ldg(PV + (long long)pl * 128 + t);
@@ -209,11 +222,11 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
     pass<C, false>(v);
     // ---- store: point (r, c) = (ar + 16 i, ac + 16 j)
     if (!CL) {
-        C* g = dst + (((long long)f0 * NQ + f1 / IL) * 64 * 64 + ar * 64 + ac) * IL + (f1 % IL);
+        S* g = dst + (((long long)f0 * NQ + f1 / IL) * 64 * 64 + ar * 64 + ac) * IL + (f1 % IL);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) g[(i * 16 * 64 + j * 16) * IL] = v[4 * i + j];
+            for (int j = 0; j < 4; ++j) g[(i * 16 * 64 + j * 16) * IL] = narrow<S>(v[4 * i + j]);
     }
     if (!KIN) {
         // observables of the new (x, p) state: p_y = ar + 16 i, p_x = ac + 16 j
@@ -270,14 +283,14 @@ k_r4(const C* __restrict__ src, C* __restrict__ dst, const double2* __restrict__
         const C* part[IL];
 #pragma unroll
         for (int g = 0; g < IL; ++g) part[g] = cl.map_shared_rank(s, g);
-        C* gb = dst + ((long long)f0 * NQ + f1 / IL) * 64 * 64 * IL;
+        S* gb = dst + ((long long)f0 * NQ + f1 / IL) * 64 * 64 * IL;
         constexpr int PER = 4096 / IL / NT;
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
             const int pt = q * (4096 / IL) + k * NT + t;
-            C val[IL];
+            S val[IL];
 #pragma unroll
-            for (int g = 0; g < IL; ++g) val[g] = part[g][pt];
+            for (int g = 0; g < IL; ++g) val[g] = narrow<S>(part[g][pt]);
             st_sector(gb + (long long)pt * IL, val);
         }
         cl.sync();                                       // partners done reading this CTA's plane

@@ -749,6 +749,8 @@ struct wig4d_plan {
     bool tc_ready;                 // k_tc64's buffers exist (wig4d_desc.transform 1 or 2)
     int tuned;                     // wig4d_autotune has set the choices above
     bool r4t_ready;                // k_r4t's tensor map and attributes are set
+    bool r4_mixed;                 // complex64 64^4: k_r4 with FP64 transforms on complex64 storage
+    void* tw64d;                   // its FP64 twiddle table
     int dense_n;                   // > 0: general-delta half-steps fused (k_dense_half, N^4 grids)
     const void* dmat[4];           // FAFT matrices per axis (|delta|), when dense_n > 0
     void* tw64;                    // k_r4 twiddle table (64 complex of the plan's dtype)
@@ -990,6 +992,7 @@ static void free_plan(wig4d_plan* p) {
     cudaFree(p->pv);
     cudaFree(p->tw64);
     cudaFree(p->fold);
+    cudaFree(p->tw64d);
     cudaFree(p->tc_bimg[0]);
     cudaFree(p->tc_bimg[1]);
     cudaFree(p->tc_pv);
@@ -1064,7 +1067,7 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
     if (!desc || !out) return WIG_ERR_INVALID_ARG;
     *out = nullptr;
     if (desc->dtype != WIG_C128 && desc->dtype != WIG_C64) return WIG_ERR_INVALID_ARG;
-    if (desc->transform < 0 || desc->transform > 2) return WIG_ERR_INVALID_ARG;
+    if (desc->transform < 0 || desc->transform > 3) return WIG_ERR_INVALID_ARG;
     for (int a = 0; a < 4; ++a) {
         if (desc->shape[a] < 2 || desc->shape[a] > 1024 || (desc->shape[a] & 1)) return WIG_ERR_UNSUPPORTED;
         if (!desc->coord[a]) return WIG_ERR_INVALID_ARG;
@@ -1335,6 +1338,18 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
         p->tc = desc->transform == 1;
         p->tc_ready = true;
     }
+    // mixed form: complex64 state, FP64 transforms and factors (k_r4<double2, ., ., float2>)
+    if (desc->transform == 3) {
+        if (desc->dtype != WIG_C64 || !p->r4) { free_plan(p); return WIG_ERR_UNSUPPORTED; }
+        if (cudaMalloc(&p->tw64d, 64 * sizeof(double2)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
+        k_make_r4_twiddles<double2><<<1, 64>>>((double2*)p->tw64d);
+        const int rsm = (int)r4_smem_bytes<double2>();
+        cudaFuncSetAttribute(k_r4<double2, true, false, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+        cudaFuncSetAttribute(k_r4<double2, false, false, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+        cudaFuncSetAttribute(k_r4<double2, true, true, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+        cudaFuncSetAttribute(k_r4<double2, false, true, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
+        p->r4_mixed = true;
+    }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { wig_set_cuda_error(e, "wig4d_plan_create"); free_plan(p); return WIG_ERR_CUDA; }
     *out = p;
@@ -1351,7 +1366,7 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     if (!p || !info) return WIG_ERR_INVALID_ARG;
     info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64;
-    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4t ? 4 : 3));
+    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? 7 : (p->r4t ? 4 : 3)));
     return WIG_OK;
 }
 
@@ -1617,12 +1632,12 @@ static int fold_and_finalize(wig4d_plan* p, double* hist, int rows, cudaStream_t
 }
 
 // k_r4 launch: with clusters of IL CTAs (full-sector stores) or plain.
-template <class C, bool KIN>
-static cudaError_t launch_r4(bool cluster, unsigned grid, size_t sm, cudaStream_t st, const C* src, C* dst,
+template <class C, bool KIN, class S = C>
+static cudaError_t launch_r4(bool cluster, unsigned grid, size_t sm, cudaStream_t st, const S* src, S* dst,
                              const double2* pv, const C* tw, double2 scale, const double* d_norm, ObsTabs ob,
                              double* partials) {
     if (!cluster) {
-        k_r4<C, KIN, false><<<grid, r4::NT, sm, st>>>(src, dst, pv, tw, scale, d_norm, ob, partials);
+        k_r4<C, KIN, false, S><<<grid, r4::NT, sm, st>>>(src, dst, pv, tw, scale, d_norm, ob, partials);
         return cudaGetLastError();
     }
     cudaLaunchConfig_t cfg = {};
@@ -1632,12 +1647,12 @@ static cudaError_t launch_r4(bool cluster, unsigned grid, size_t sm, cudaStream_
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = r4::Il<C>::v;
+    attr[0].val.clusterDim.x = r4::Il<S>::v;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_r4<C, KIN, true>, src, dst, pv, tw, scale, d_norm, ob, partials);
+    return cudaLaunchKernelEx(&cfg, k_r4<C, KIN, true, S>, src, dst, pv, tw, scale, d_norm, ob, partials);
 }
 
 template <class C>
@@ -1683,6 +1698,30 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
                                                           make_double2(p->pot_scale, 0.0), p->cur_norm, p->ob,
                                                           p->partials);
                 WIG_LAUNCHED("k_r4t<pot>");
+            } else {
+                return fold_and_finalize(p, hist, rows, st);
+            }
+            return WIG_OK;
+        }
+    }
+    if constexpr (std::is_same<C, float2>::value) {
+        if (p->r4 && p->r4_mixed) {
+            // complex64 LA / LB layouts, FP64 transforms
+            float2* P = reinterpret_cast<float2*>(p->pingpong);
+            const double2* pv = reinterpret_cast<const double2*>(p->pv);
+            constexpr size_t sm = r4_smem_bytes<double2>();
+            const double2* tw = reinterpret_cast<const double2*>(p->tw64d);
+            if (part == 0) {
+                WIG_CUDA((launch_r4<double2, true, float2>(p->r4_cluster, 64 * 64, sm, st, P, W, pv, tw,
+                                                           make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob,
+                                                           nullptr)));
+                WIG_LAUNCHED("k_r4<double2, kin, float2>");
+            } else if (part == 1) {
+                WIG_CUDA((launch_r4<double2, false, float2>(p->r4_cluster, 64 * 64, sm, st, W, P,
+                                                            pv + (size_t)p->shape[0] * p->shape[2] * 128, tw,
+                                                            make_double2(p->pot_scale, 0.0), nullptr, p->ob,
+                                                            p->partials)));
+                WIG_LAUNCHED("k_r4<double2, pot, float2>");
             } else {
                 return fold_and_finalize(p, hist, rows, st);
             }

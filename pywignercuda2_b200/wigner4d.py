@@ -22,6 +22,8 @@ Extra attributes a frame may set (defaults reproduce the reference):
   64-point transforms as dense FAFT GEMMs on the tensor cores (fp16 hi + lo
   operands, FP32 accumulation; k_tc64) instead of the CUDA-core kernels;
   "auto" makes them a candidate of the autotuner.
+* ``fp64_transforms``: True (complex64 64^4 grids, delta = 1/N) keeps the
+  complex64 state in memory but runs the transforms and factors in FP64.
 * ``autotune``: True times the plan's kernel choices once per (grid, dtype,
   kernel path) in the process (wig4d_autotune) and keeps the fastest; the
   choice is in ``self.autotune_choice``.  "force" times it again.
@@ -58,6 +60,7 @@ class GPU_Wigner4D:
     round_constants = True
     tensor_cores = False
     autotune = False
+    fp64_transforms = False
 
     def __init__(self):
         require_cuda()
@@ -178,7 +181,10 @@ class GPU_Wigner4D:
         d.dv_norm = self.dx * self.dp_x * self.dy * self.dp_y
         d.dv_obs = self._c("dx") * self._c("dy") * self._c("dp_x") * self._c("dp_y")
         plan = ctypes.c_void_p()
-        d.transform = 2 if self.tensor_cores == "auto" else (1 if self.tensor_cores else 0)
+        if self.fp64_transforms:
+            d.transform = 3
+        else:
+            d.transform = 2 if self.tensor_cores == "auto" else (1 if self.tensor_cores else 0)
         _lib.call("wig4d_plan_create", ctypes.byref(d), ctypes.byref(plan))
         self._plan = plan
         self.autotune_choice = None
@@ -339,7 +345,7 @@ class GPU_Wigner4D:
         """Kernels the plan runs: fused_kinetic, fused_potential, fast64, run64_kernel."""
         info = (ctypes.c_int * 4)()
         _lib.call("wig4d_plan_info", self._plan, info)
-        run64 = {0: None, 3: "r4", 4: "r4t", 6: "tc"}[info[3]]
+        run64 = {0: None, 3: "r4", 4: "r4t", 6: "tc", 7: "r4_mixed"}[info[3]]
         return {"fused_kinetic": bool(info[0]), "fused_potential": bool(info[1]), "fast64": bool(info[2]),
                 "run64_kernel": run64}
 

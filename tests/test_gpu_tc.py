@@ -105,3 +105,20 @@ def test_tc_rejects_unsupported_plans(dtype, n):
     with pytest.raises(_lib.WignerError) as e:
         make_frame(GPU_Wigner4D, p, complex_dtype=dtype, tensor_cores=True)
     assert e.value.status == 2
+
+
+def test_mixed_form_vs_oracle_20_iterations_64():
+    """complex64 storage with FP64 transforms (fp64_transforms = True): the
+    only rounding left is the state's float32 storage, relative to each
+    value, so the energy stays within 1e-6 of the oracle."""
+    p, c = config2(0, 64)
+    o = Wigner4DOracle(p)
+    f = make_frame(GPU_Wigner4D, p, complex_dtype=np.complex64, fp64_transforms=True)
+    assert f.plan_info()["run64_kernel"] == "r4_mixed"
+    W0 = cat_xp(f._coords, c)
+    Wo, obs = o.run(W0.astype(np.complex64).astype(np.complex128), 19)
+    f = _run(p, W0, 20, complex_dtype=np.complex64, fp64_transforms=True)
+    for name in OBS:
+        assert rel_err(getattr(f, name), obs[name]) < 1e-6, name
+    assert rel_err(f.norm, obs["norms"]) < 1e-9
+    assert rel_err(f.W_init_gpu.get(), Wo) < 1e-6
