@@ -346,6 +346,31 @@ def bench_dirac(steps):
                     "finite": bool(np.all(np.isfinite(f.energyKinetic)))}
     out["pass_ms"] = dirac_passes(f)
     del f
+    torch.cuda.empty_cache()
+    # the complex64 form of the same workload (fused loop), beside the plain one
+    f, _, _ = _dirac_frame(steps, np.complex64)
+    Ws = [getattr(f, k) for k in NAMES]
+    f.alias_w21 = False
+
+    def init32():
+        f.WignerDiracGaussian_ParticleUp_GPU(*Ws, 0.0, 0.0, x0, y0, 1.0, 1.0)
+        f._Fourier_Theta_To_P_64_64_4x4_GPU(*Ws)
+    init32()
+    f.timeSteps = 1
+    f.Run()
+    init32()
+    f.timeSteps = steps - 1
+    torch.cuda.synchronize()
+    e0.record()
+    f.Run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["fused_loop_c64"] = {"steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps,
+                             "state_bytes": 16 * n ** 4 * 8,
+                             "finite": bool(np.all(np.isfinite(f.energyKinetic))),
+                             "energy_kinetic_last": float(f.energyKinetic[-1])}
+    del f
     return out
 
 
