@@ -266,7 +266,8 @@ int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
    3 k_r4 (16 points per thread, the default), 4 k_r4t (complex128 k_r4 with
    TMA plane loads, WIG_FAST64_KERNEL=r4t), 6 k_tc64 (tensor-core transforms,
    wig4d_desc.transform = 1), 7 k_r4 with FP64 transforms on complex64
-   storage (wig4d_desc.transform = 3). */
+   storage (wig4d_desc.transform = 3), 8 k_r4ring (complex128 persistent
+   k_r4 with a TMA ring of planes, WIG_FAST64_KERNEL=r4ring). */
 int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
 
 
@@ -275,14 +276,14 @@ int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
  * kernel choices this plan has on a scratch copy of a Gaussian state
  * (`iterations` Run() iterations each, CUDA events on `stream`) and keeps
  * the fastest.  The candidates are the 64^4 engines (k_r4 with cluster or
- * plain stores, complex128 k_r4t, and k_tc64 when the plan was made with
+ * plain stores, complex128 k_r4t and k_r4ring, and k_tc64 when the plan was made with
  * wig4d_desc.transform = 2) or, for the other kernels, k_kin48 against
  * k_kinetic on 48 x 48 planes and the columns per CTA of k_potential_g
  * (8, 4, 2, or k_potential).  The choice is cached per (shape, dtype,
  * kernel path) for the process: later plans with the same key take it
  * without timing unless flags has WIG_TUNE_FORCE.  choice_out (host, 4
  * ints, may be NULL) receives the engine (0 k_r4 plain, 1 k_r4 cluster,
- * 2 k_r4t, 3 k_tc64, 4 the per-size kernels), k_kin48 (1/0), the columns
+ * 2 k_r4t, 3 k_tc64, 4 the per-size kernels, 5 k_r4ring), k_kin48 (1/0), the columns
  * per CTA and the number of candidates timed.  Allocates a scratch state;
  * synchronous; call it outside any stream capture.
  */

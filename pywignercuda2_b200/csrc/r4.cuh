@@ -54,19 +54,50 @@ template <class C, bool FWD> __device__ __forceinline__ void pass(C (&v)[16]) {
     for (int j = 0; j < 4; ++j) dft4<C, FWD>(v[j], v[4 + j], v[8 + j], v[12 + j]);
 }
 
+// Slot of w^k (k < 16) in the complex128 shared table: with k's bits b0..b3,
+// slot = b0 + 2 b2 + 4 (b1 ^ b3) + 8 b3, so that every quarter-warp of the
+// four twiddle calls (a = t & 15, 4 (t & 3), (t >> 2 & 3) + 4 (t & 3),
+// 4 (t >> 2 & 3) and the warp-uniform b) reads distinct 16-byte bank groups.
+__device__ __forceinline__ int tw_slot(int k) {
+    return (k & 1) | ((k >> 1) & 2) | ((((k >> 1) ^ (k >> 3)) & 1) << 2) | (k & 8);
+}
+// fill the shared twiddle table from the plan's table gtw[k] = w^k
+__device__ __forceinline__ void load_tw(double2* tw, const double2* gtw, int t) {
+    if (t < 16) tw[tw_slot(t)] = gtw[t];
+}
+__device__ __forceinline__ void load_tw(float2* tw, const float2* gtw, int t) {
+    if (t < 64) tw[t] = gtw[t];
+}
+// w^a, w^2a, w^3a (a <= 15).  complex128: one table load, the square and the
+// cube in FP64 (a few units in the last place); a 128-bit shared load is
+// served per quarter-warp, so three loads of scattered entries cost several
+// times the wavefronts of one.  complex64: the table's normalised entries
+// (|w|^2 closest to 1), which a float32 recurrence would not keep.
+__device__ __forceinline__ void tw_powers(const double2* tw, int a, double2 (&w)[3]) {
+    w[0] = tw[tw_slot(a)];
+    w[1] = make_double2(fma(w[0].x, w[0].x, -w[0].y * w[0].y), (2.0 * w[0].x) * w[0].y);
+    w[2] = zmul(w[1], w[0]);
+}
+__device__ __forceinline__ void tw_powers(const float2* tw, int a, float2 (&w)[3]) {
+    w[0] = tw[a];
+    w[1] = tw[2 * a];
+    w[2] = tw[3 * a];
+}
+
 // v[i][j] *= w^(a j + b i) (FWD) or its conjugate, w = exp(-2 pi i / 64)
 template <class C, bool FWD> __device__ __forceinline__ void twiddle(C (&v)[16], const C* tw, int a, int b) {
+    C wa[3], wb[3];
+    tw_powers(tw, a, wa);
+    tw_powers(tw, b, wb);
 #pragma unroll
     for (int j = 1; j < 4; ++j) {
-        C w = tw[a * j];
-        if (!FWD) w = cconj(w);
+        const C w = FWD ? wa[j - 1] : cconj(wa[j - 1]);
 #pragma unroll
         for (int i = 0; i < 4; ++i) v[4 * i + j] = cmul(v[4 * i + j], w);
     }
 #pragma unroll
     for (int i = 1; i < 4; ++i) {
-        C w = tw[b * i];
-        if (!FWD) w = cconj(w);
+        const C w = FWD ? wb[i - 1] : cconj(wb[i - 1]);
 #pragma unroll
         for (int j = 0; j < 4; ++j) v[4 * i + j] = cmul(v[4 * i + j], w);
     }
@@ -174,8 +205,10 @@ k_r4(const S* __restrict__ src, S* __restrict__ dst, const double2* __restrict__
             for (int j = 0; j < 4; ++j)
                 v[4 * i + j] = widen<C>(g[(long long)i * (16LL * 64 * 64 * 64) + (long long)j * (16LL * 64 * 64)]);
     }
-    if (t < 64) tw[t] = gtw[t];
-    if (t < 128) pvs[t] = __ldg(PV + (long long)pl * 128 + t);
+    load_tw(tw, gtw, t);
+    // row vector as is; column entry kc at 64 + (kc & 48) + 4 (kc & 3) + (kc >> 2 & 3),
+    // so that each quarter-warp's column factors lie in distinct bank groups
+    if (t < 128) pvs[t < 64 ? t : 64 + (t & 48) + ((t & 3) << 2) + ((t >> 2) & 3)] = __ldg(PV + (long long)pl * 128 + t);
     double2 cc = scale;
     if (KIN && d_norm) cc = zmul(cc, zinv(make_double2(d_norm[0], d_norm[1])));
     const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
@@ -198,7 +231,7 @@ k_r4(const S* __restrict__ src, S* __restrict__ dst, const double2* __restrict__
         const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
         double2 b[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = pvs[64 + c2 + 4 * c1 + 16 * j];
+        for (int j = 0; j < 4; ++j) b[j] = pvs[64 + 16 * j + 4 * c2 + c1];     // column kc = c2 + 4 c1 + 16 j
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const double2 a = zmul(pvs[r2 + 4 * r1 + 16 * i], cc);
@@ -395,7 +428,7 @@ k_r4t(const __grid_constant__ CUtensorMap src_map, double2* __restrict__ dst,
         mbar_expect_tx(bar, 64 * 64 * sizeof(C));
         tma_load_5d(s, &src_map, 0, f1, f0, 0, 0, bar);
     }
-    if (t < 64) tw[t] = gtw[t];
+    load_tw(tw, gtw, t);
     double2 cc = scale;
     if (KIN) cc = zmul(cc, zinv(make_double2(d_norm[0], d_norm[1])));
     __syncthreads();                                   // barrier initialised before anyone waits
@@ -503,6 +536,269 @@ k_r4t(const __grid_constant__ CUtensorMap src_map, double2* __restrict__ dst,
     }
 }
 
+// ---------------------------------------------------------------------------
+// k_r4ring: the 64^4 half-steps of k_r4 as a persistent kernel whose planes
+// stream through a ring of shared-memory buffers filled by TMA.
+//
+// One CTA per SM holds NG = IL plane groups of 256 threads (2 for
+// complex128, 4 for complex64) and NB = NG + 1 plane buffers.  The CTA
+// walks the units u = blockIdx.x, blockIdx.x + gridDim.x, ...; a unit is the
+// IL planes f1 = IL m .. IL m + IL - 1 of one f0 that share every
+// destination sector, so the IL groups store the halves (quarters) of the
+// same sectors at about the same time.  Local plane k (plane k % IL of the
+// CTA's unit k / IL) belongs to group k % NG and lives in buffer k % NB.
+//
+// A buffer is refilled with local plane k + NB by one thread of the group
+// that used it for plane k, as soon as that group has read its last
+// exchange out of it; the group then runs its last inverse pass, the
+// observables and the stores from registers while the copy is in flight.
+// Every group's next plane has therefore been loading since the group
+// before it released a buffer, and no thread issues a global load of the
+// state.  A plane lands in natural [r][c] order (the box of k_r4t), is read
+// straight into layout L1, and its buffer then serves as the exchange plane.
+// Exchanges and arithmetic are k_r4's, on one named barrier per group.
+//
+// Each copy completes on its buffer's mbarrier (bytes counted).  Waits are
+// bounded and the group decides together (bar.red.and) whether its plane
+// arrived; if not, it poisons the norm (kinetic) or the plane's partial row
+// (potential) with NaN, raises the CTA's abort word (other groups stop at
+// their next wait), and before the CTA exits one thread waits, bounded
+// again, for every copy it issued.
+// ---------------------------------------------------------------------------
+namespace r4ring {
+
+template <class C> struct Cfg {
+    static constexpr int IL = r4::Il<C>::v, NG = IL, NB = NG + 1, NTH = NG * r4::NT;
+    static constexpr size_t PLANE = 64 * 64 * sizeof(C);
+    static constexpr size_t TW_OFF = NB * PLANE;                           // 64 twiddles
+    static constexpr size_t PV_OFF = TW_OFF + 64 * sizeof(C);              // per group: 128 FP64 factors
+    static constexpr size_t RED_OFF = PV_OFF + NG * 128 * sizeof(double2); // per group: 8 warps x 16 slots
+    static constexpr size_t BAR_OFF = RED_OFF + NG * 8 * 16 * sizeof(double);
+    static constexpr size_t CNT_OFF = BAR_OFF + NB * sizeof(uint64_t);     // copies issued per buffer, abort
+    static constexpr size_t SMEM = CNT_OFF + 16 * sizeof(int) + 128;       // + alignment of the base
+    static_assert(SMEM <= 232448, "k_r4ring shared memory");
+};
+
+__device__ __forceinline__ void group_sync(int g) { asm volatile("bar.sync %0, 256;" ::"r"(1 + g) : "memory"); }
+
+// true on every thread of group g iff p holds on all of them
+__device__ __forceinline__ bool group_all(bool p, int g) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred q, d;\n setp.ne.u32 q, %1, 0;\n bar.red.and.pred d, %2, 256, q;\n selp.u32 %0, 1, 0, d;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)p), "r"(1 + g)
+        : "memory");
+    return r != 0;
+}
+
+// Bounded wait for use n of a buffer (its (n+1)-th copy).  A parity wait
+// alone cannot tell phase n from phase n - 2: a group may reach use n while
+// the buffer still holds (or awaits) use n - 1 of another group.  So first
+// wait until the copy of use n has been issued (issued > n), which happens
+// only after use n - 1 has landed and been consumed; then the parity of
+// phase n is unambiguous.  Gives up early once the CTA's abort word is set.
+__device__ __forceinline__ bool wait_plane(uint64_t* bar, const volatile int* issued, int n,
+                                           const volatile int* abort_word) {
+    int it = 0;
+    for (; it < (1 << 22); ++it) {
+        if (*issued > n) break;
+        if ((it & 1023) == 1023 && *abort_word) return false;
+    }
+    for (; it < (1 << 22); ++it) {
+        if (r4t::mbar_try_wait(bar, (uint32_t)(n & 1))) return true;
+        if ((it & 1023) == 1023 && *abort_word) return false;
+    }
+    return false;
+}
+
+// Sum of 16 per-lane values over the warp, transposed: after the call a[0]
+// on lane l holds the warp's total of slot (l >> 1) & 15 (4 halving levels
+// of xor-shuffles that each move half of the remaining slots, then one of
+// plain addition), 32 shuffles of doubles in all.
+__device__ __forceinline__ double warp_slot_sums(double (&a)[16], int lane) {
+#pragma unroll
+    for (int lv = 0; lv < 4; ++lv) {
+        const int h = 8 >> lv, m = 16 >> lv;
+        const bool up = (lane & m) != 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if (q < h) {
+                const double send = up ? a[q] : a[q + h];
+                const double keep = up ? a[q + h] : a[q];
+                a[q] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+            }
+        }
+    }
+    return a[0] + __shfl_xor_sync(0xffffffffu, a[0], 1);
+}
+
+}  // namespace r4ring
+
+template <class C, bool KIN>
+__global__ void __launch_bounds__(r4ring::Cfg<C>::NTH, 1)
+k_r4ring(const __grid_constant__ CUtensorMap src_map, C* __restrict__ dst, const double2* __restrict__ PV,
+         const C* __restrict__ gtw, double2 scale, double* __restrict__ d_norm, ObsTabs ob,
+         double* __restrict__ partials) {
+    using namespace r4;
+    using namespace r4t;
+    using namespace r4ring;
+    typedef Cfg<C> K;
+    constexpr int IL = K::IL, NG = K::NG, NB = K::NB, NQ = 64 / IL;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+    C* tw = reinterpret_cast<C*>(base + K::TW_OFF);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + K::BAR_OFF);
+    volatile int* issued = reinterpret_cast<int*>(base + K::CNT_OFF);  // [NB] copies per buffer, [NB] abort word
+    volatile int* abort_word = issued + NB;
+    const int tid = threadIdx.x, g = tid >> 8, t = tid & (NT - 1), lane = t & 31, wp = t >> 5;
+    double2* pvs = reinterpret_cast<double2*>(base + K::PV_OFF) + g * 128;
+    double* red = reinterpret_cast<double*>(base + K::RED_OFF) + g * 128;
+    const int nunits = 4096 / IL;
+    const int nloc = (int)blockIdx.x < nunits ? ((nunits - 1 - (int)blockIdx.x) / (int)gridDim.x + 1) * IL : 0;
+    auto plane_of = [&](int k) { return ((int)blockIdx.x + (k / IL) * (int)gridDim.x) * IL + k % IL; };
+    if (tid == 0) {
+        for (int b = 0; b < NB; ++b) {
+            mbar_init(bars + b);
+            issued[b] = 0;
+        }
+        issued[NB] = 0;
+        issued[NB + 1] = 0;                            // stays 0: the final drain never gives up early
+        fence_async_smem();
+        for (int k = 0; k < NB && k < nloc; ++k) {
+            const int pl = plane_of(k);
+            mbar_expect_tx(bars + k, (uint32_t)K::PLANE);
+            tma_load_5d(base + k * K::PLANE, &src_map, 0, pl & 63, pl >> 6, 0, 0, bars + k);
+            issued[k] = 1;
+        }
+    }
+    if (tid < 64) load_tw(tw, gtw, tid);
+    double2 cc = scale;
+    if (KIN) cc = zmul(cc, zinv(make_double2(d_norm[0], d_norm[1])));
+    const int ac = t & 15, ar = t >> 4;
+    const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
+    __syncthreads();                                   // barriers, counters and twiddles ready
+    for (int k = g; k < nloc; k += NG) {
+        const int bf = k % NB, pl = plane_of(k), f0 = pl >> 6, f1 = pl & 63;
+        C* s = reinterpret_cast<C*>(base + bf * K::PLANE);
+        // this plane's factor vectors (first read after the exchanges' barriers;
+        // column entry kc at 64 + (kc & 48) + 4 (kc & 3) + (kc >> 2 & 3))
+        if (t < 128) pvs[t < 64 ? t : 64 + (t & 48) + ((t & 3) << 2) + ((t >> 2) & 3)] = __ldg(PV + (long long)pl * 128 + t);
+        const bool arrived = wait_plane(bars + bf, issued + bf, k / NB, abort_word);
+        if (!group_all(arrived, g)) {
+            if (t == 0) {
+                if (KIN) d_norm[0] = __longlong_as_double(0x7ff8000000000000LL);
+                else partials[(long long)pl * NPART] = __longlong_as_double(0x7ff8000000000000LL);
+                *abort_word = 1;
+            }
+            break;
+        }
+        C v[16];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[4 * i + j] = s[(ar + 16 * i) * 64 + ac + 16 * j];
+        // ---- forward
+        pass<C, true>(v);
+        twiddle<C, true>(v, tw, ac, ar);
+        group_sync(g);                                 // the landed plane has been read
+        put(s, L1, v);
+        group_sync(g);
+        get(s, L2, v);
+        pass<C, true>(v);
+        twiddle<C, true>(v, tw, 4 * (t & 3), 4 * ((t >> 4) & 3));
+        group_sync(g);
+        put(s, L2, v);
+        group_sync(g);
+        get(s, L3, v);
+        pass<C, true>(v);
+        {
+            const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
+            double2 b[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = pvs[64 + 16 * j + 4 * c2 + c1];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const double2 a = zmul(pvs[r2 + 4 * r1 + 16 * i], cc);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) factor_mul(v[4 * i + j], a, b[j]);
+            }
+        }
+        // ---- inverse
+        pass<C, false>(v);
+        twiddle<C, false>(v, tw, ((t >> 2) & 3) + 4 * (t & 3), (t >> 6) + 4 * ((t >> 4) & 3));
+        group_sync(g);
+        put(s, L3, v);
+        group_sync(g);
+        get(s, L2, v);
+        pass<C, false>(v);
+        twiddle<C, false>(v, tw, 4 * ((t >> 2) & 3), 4 * (t >> 6));
+        group_sync(g);
+        put(s, L2, v);
+        group_sync(g);
+        get(s, L1, v);
+        group_sync(g);                                 // the group is done with the buffer
+        if (t == 0 && k + NB < nloc) {
+            const int pn = plane_of(k + NB);
+            fence_async_smem();
+            mbar_expect_tx(bars + bf, (uint32_t)K::PLANE);
+            tma_load_5d(s, &src_map, 0, pn & 63, pn >> 6, 0, 0, bars + bf);
+            issued[bf] += 1;
+        }
+        pass<C, false>(v);
+        // ---- store: point (r, c) = (ar + 16 i, ac + 16 j), one IL-th of each sector
+        {
+            C* gd = dst + (((long long)f0 * NQ + f1 / IL) * 64 * 64 + ar * 64 + ac) * IL + (f1 % IL);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) gd[(i * 16 * 64 + j * 16) * IL] = v[4 * i + j];
+        }
+        if (!KIN) {
+            // observables of the new (x, p) state: p_y = ar + 16 i, p_x = ac + 16 j
+            typedef typename real_of<C>::type R;
+            R a[NPART];
+#pragma unroll
+            for (int q = 0; q < NPART; ++q) a[q] = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const R qy = (R)__ldg(ob.cpy + ar + 16 * i);
+                R w0x = 0, w0y = 0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const C w = v[4 * i + j];
+                    const R qx = (R)__ldg(ob.cpx + ac + 16 * j), kk = (R)__ldg(ob.ep + (ar + 16 * i) * 64 + ac + 16 * j);
+                    w0x += w.x; w0y += w.y;
+                    a[2] += qx * w.x; a[3] += qx * w.y;
+                    a[4] += qx * qx * w.x; a[5] += qx * qx * w.y;
+                    a[10] += kk * w.x; a[11] += kk * w.y;
+                }
+                a[0] += w0x; a[1] += w0y;
+                a[6] += qy * w0x; a[7] += qy * w0y;
+                a[8] += qy * qy * w0x; a[9] += qy * qy * w0y;
+            }
+            double d[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) d[q] = q < NPART ? (double)a[q] : 0.0;
+            const double sum = warp_slot_sums(d, lane);
+            if (!(lane & 1)) red[wp * 16 + (lane >> 1)] = sum;
+            group_sync(g);
+            if (t < NPART) {
+                double tot = 0.0;
+#pragma unroll
+                for (int w = 0; w < NT / 32; ++w) tot += red[w * 16 + t];
+                partials[(long long)pl * NPART + t] = tot;
+            }
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && *abort_word) {
+        // no copy may still target this CTA's shared memory when it exits
+        for (int b = 0; b < NB; ++b)
+            if (issued[b] > 0) wait_plane(bars + b, issued + b, issued[b] - 1, issued + NB + 1);
+    }
+}
+
 // The 64-entry twiddle table of k_r4 / k_r4t, built once per plan.
 template <class C>
 __global__ void k_make_r4_twiddles(C* tw) { r4::make_tw<C>(tw); }
@@ -548,7 +844,7 @@ k_dplane_r4(PlaneSlots<C> S, const C* __restrict__ gtw, double2 scale, const dou
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) v[4 * i + j] = g[(ar + 16 * i) * rs + (ac + 16 * j) * cs];
-    if (t < 64) tw[t] = gtw[t];
+    load_tw(tw, gtw, t);
     double2 sc = scale;
     if (d_norm) sc = zmul(sc, zinv(make_double2(d_norm[0], d_norm[1])));
     const C cc = to_c<C>(sc);
@@ -635,7 +931,7 @@ k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, PlaneSlots<C> S, const C
         r4t::mbar_expect_tx(bar, 65536);
         dpt::tma_load_4d(s, map, 2 * GP * m, 0, i1, 0, bar);
     }
-    if (threadIdx.x < 64) tw[threadIdx.x] = gtw[threadIdx.x];
+    load_tw(tw, gtw, threadIdx.x);
     double2 sc = scale;
     if (d_norm) sc = zmul(sc, zinv(make_double2(d_norm[0], d_norm[1])));
     const C cc = to_c<C>(sc);

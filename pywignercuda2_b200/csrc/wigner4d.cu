@@ -749,6 +749,8 @@ struct wig4d_plan {
     bool tc_ready;                 // k_tc64's buffers exist (wig4d_desc.transform 1 or 2)
     int tuned;                     // wig4d_autotune has set the choices above
     bool r4t_ready;                // k_r4t's tensor map and attributes are set
+    bool r4ring;                   // complex128 64^4 Run(): persistent k_r4ring (TMA plane ring)
+    bool r4ring_ready;             // k_r4ring's tensor map and attributes are set
     bool r4_mixed;                 // complex64 64^4: k_r4 with FP64 transforms on complex64 storage
     void* tw64d;                   // its FP64 twiddle table
     int dense_n;                   // > 0: general-delta half-steps fused (k_dense_half, N^4 grids)
@@ -1063,6 +1065,18 @@ static int ensure_r4t(wig4d_plan* p) {
     return WIG_OK;
 }
 
+// k_r4ring (complex128): the same LA map of the ping-pong buffer as k_r4t.
+static int ensure_r4ring(wig4d_plan* p) {
+    if (p->r4ring_ready) return WIG_OK;
+    int r;
+    if ((r = ensure_r4t(p))) return r;
+    const int sm = (int)r4ring::Cfg<double2>::SMEM;
+    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    p->r4ring_ready = true;
+    return WIG_OK;
+}
+
 extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
     if (!desc || !out) return WIG_ERR_INVALID_ARG;
     *out = nullptr;
@@ -1256,13 +1270,19 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             if (!ok) { wig_set_cuda_error(cudaGetLastError(), "plane vectors"); free_plan(p); return WIG_ERR_CUDA; }
         }
         // k_r4 with cluster stores (default); WIG_FAST64_KERNEL = r4 (plain
-        // stores) or r4t (complex128 TMA plane loads)
+        // stores), r4t (complex128 TMA plane loads) or r4ring (complex128
+        // persistent TMA ring)
         const char* kern = getenv("WIG_FAST64_KERNEL");
         p->r4 = true;
         if (desc->dtype == WIG_C128 && kern && strcmp(kern, "r4t") == 0) {
             int r;
             if ((r = ensure_r4t(p))) { free_plan(p); return r; }
             p->r4t = true;
+        }
+        if (desc->dtype == WIG_C128 && kern && strcmp(kern, "r4ring") == 0) {
+            int r;
+            if ((r = ensure_r4ring(p))) { free_plan(p); return r; }
+            p->r4ring = true;
         }
         p->r4_cluster = !(kern && strcmp(kern, "r4") == 0);
         if (cudaMalloc(&p->tw64, 64 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
@@ -1366,7 +1386,7 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     if (!p || !info) return WIG_ERR_INVALID_ARG;
     info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64;
-    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? 7 : (p->r4t ? 4 : 3)));
+    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? 7 : (p->r4ring ? 8 : (p->r4t ? 4 : 3))));
     return WIG_OK;
 }
 
@@ -1681,6 +1701,28 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
         }
     }
     if constexpr (std::is_same<C, double2>::value) {
+        if (p->r4ring) {
+            int s;
+            if ((s = ensure_w_maps(p, W))) return s;
+            const double2* pv = reinterpret_cast<const double2*>(p->pv);
+            typedef r4ring::Cfg<double2> K;
+            const unsigned grid = (unsigned)(wig_num_sms() < 4096 / K::IL ? wig_num_sms() : 4096 / K::IL);
+            // kinetic: LA (ping-pong) -> LB (W); potential: LB (W) -> LA (ping-pong)
+            if (part == 0) {
+                k_r4ring<double2, true><<<grid, K::NTH, K::SMEM, st>>>(p->map_t_load, W, pv, (const double2*)p->tw64,
+                                                                       make_double2(p->kin_scale, 0.0), p->cur_norm,
+                                                                       p->ob, nullptr);
+                WIG_LAUNCHED("k_r4ring<kin>");
+            } else if (part == 1) {
+                k_r4ring<double2, false><<<grid, K::NTH, K::SMEM, st>>>(
+                    p->map_w_load, reinterpret_cast<double2*>(p->pingpong), pv + (size_t)p->shape[0] * p->shape[2] * 128,
+                    (const double2*)p->tw64, make_double2(p->pot_scale, 0.0), p->cur_norm, p->ob, p->partials);
+                WIG_LAUNCHED("k_r4ring<pot>");
+            } else {
+                return fold_and_finalize(p, hist, rows, st);
+            }
+            return WIG_OK;
+        }
         if (p->r4t) {
             int s;
             if ((s = ensure_w_maps(p, W))) return s;
@@ -1863,15 +1905,20 @@ struct TuneKey {
 struct TuneChoice { int engine, kin48, pot_gmax; };
 
 // engine: 0 k_r4 plain stores, 1 k_r4 cluster stores, 2 k_r4t, 3 k_tc64,
-// 4 the CUDA-core path of a plan without the 64^4 radix kernels
+// 4 the CUDA-core path of a plan without the 64^4 radix kernels, 5 k_r4ring
 int apply_choice(wig4d_plan* p, const TuneChoice& c) {
     if (c.engine == 2) {
         const int r = ensure_r4t(p);
         if (r) return r;
     }
+    if (c.engine == 5) {
+        const int r = ensure_r4ring(p);
+        if (r) return r;
+    }
     p->tc = c.engine == 3;
     p->r4_cluster = c.engine == 1;
     p->r4t = c.engine == 2;
+    p->r4ring = c.engine == 5;
     p->kin48 = c.kin48 != 0;
     p->pot_gmax = c.pot_gmax;
     if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
@@ -1880,7 +1927,7 @@ int apply_choice(wig4d_plan* p, const TuneChoice& c) {
 
 TuneChoice current_choice(const wig4d_plan* p) {
     TuneChoice c;
-    c.engine = p->tc ? 3 : (p->r4 ? (p->r4t ? 2 : (p->r4_cluster ? 1 : 0)) : 4);
+    c.engine = p->tc ? 3 : (p->r4 ? (p->r4ring ? 5 : (p->r4t ? 2 : (p->r4_cluster ? 1 : 0))) : 4);
     c.kin48 = p->kin48;
     c.pot_gmax = p->pot_gmax;
     return c;
@@ -1918,6 +1965,7 @@ extern "C" int wig4d_autotune(wig4d_plan* p, int iterations, int flags, void* st
         engines.push_back({1, base.kin48, base.pot_gmax});
         engines.push_back({0, base.kin48, base.pot_gmax});
         if (p->dtype == WIG_C128) engines.push_back({2, base.kin48, base.pot_gmax});
+        if (p->dtype == WIG_C128) engines.push_back({5, base.kin48, base.pot_gmax});
     } else {
         engines.push_back({4, base.kin48, base.pot_gmax});
     }

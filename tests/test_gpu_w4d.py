@@ -302,10 +302,12 @@ def test_k48_matches_generic(dtype, tol, monkeypatch):
         assert rel_err(a, b) < tol
 
 
-@pytest.mark.parametrize("variant", ["r4t", "r4"])
+@pytest.mark.parametrize("variant", ["r4t", "r4", "r4ring"])
 def test_r4_variants_match_default(variant, monkeypatch):
-    """complex128: k_r4 with TMA plane loads (r4t) and k_r4 with plain stores
-    (r4) against the default k_r4 with cluster stores: the same arithmetic."""
+    """complex128: k_r4 with TMA plane loads (r4t), k_r4 with plain stores
+    (r4) and the persistent k_r4ring (TMA ring of planes) against the default
+    k_r4 with cluster stores: the same arithmetic (k_r4ring sums each plane's
+    observables in another order)."""
     from configs import cat_xp
     p, c = config2(7, 64)
     f1 = make_frame(GPU_Wigner4D, p)
