@@ -612,6 +612,18 @@ __device__ __forceinline__ bool wait_plane(uint64_t* bar, const volatile int* is
     return false;
 }
 
+// TMA tensor store of one plane from shared memory (bulk group of the
+// issuing thread), and the waits for its reads of shared memory / for all of it
+__device__ __forceinline__ void tma_store_5d(const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+                                             const void* src) {
+    asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];"
+                 ::"l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(r4t::sa(src))
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // Sum of 16 per-lane values over the warp, transposed: after the call a[0]
 // on lane l holds the warp's total of slot (l >> 1) & 15 (4 halving levels
 // of xor-shuffles that each move half of the remaining slots, then one of
@@ -635,11 +647,17 @@ __device__ __forceinline__ double warp_slot_sums(double (&a)[16], int lane) {
 
 }  // namespace r4ring
 
-template <class C, bool KIN>
+// TS: the result leaves by one TMA tensor store per plane (dst_map, box
+// (2 reals, 1, 64, 64, 1) at (0, f1 % IL, 0, 0, unit)) from the plane's
+// buffer, written there in natural [r][c] order; the buffer's refill then
+// waits until the store has read it, which the group's thread 0 checks at
+// the group's next plane (after reading its input) or after its last plane.
+// Without TS each thread stores its 16 points (one IL-th of 16 sectors).
+template <class C, bool KIN, bool TS>
 __global__ void __launch_bounds__(r4ring::Cfg<C>::NTH, 1)
-k_r4ring(const __grid_constant__ CUtensorMap src_map, C* __restrict__ dst, const double2* __restrict__ PV,
-         const C* __restrict__ gtw, double2 scale, double* __restrict__ d_norm, ObsTabs ob,
-         double* __restrict__ partials) {
+k_r4ring(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map,
+         C* __restrict__ dst, const double2* __restrict__ PV, const C* __restrict__ gtw, double2 scale,
+         double* __restrict__ d_norm, ObsTabs ob, double* __restrict__ partials) {
     using namespace r4;
     using namespace r4t;
     using namespace r4ring;
@@ -677,6 +695,17 @@ k_r4ring(const __grid_constant__ CUtensorMap src_map, C* __restrict__ dst, const
     if (KIN) cc = zmul(cc, zinv(make_double2(d_norm[0], d_norm[1])));
     const int ac = t & 15, ar = t >> 4;
     const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
+    // thread 0 of a group: refill buffer (k + NB) % NB with local plane k + NB
+    auto refill = [&](int kk) {
+        if (kk + NB < nloc) {
+            const int b = kk % NB, pn = plane_of(kk + NB);
+            fence_async_smem();
+            mbar_expect_tx(bars + b, (uint32_t)K::PLANE);
+            tma_load_5d(base + b * K::PLANE, &src_map, 0, pn & 63, pn >> 6, 0, 0, bars + b);
+            issued[b] += 1;
+        }
+    };
+    int pend = -1;                                     // TS, thread 0: plane whose buffer awaits its refill
     __syncthreads();                                   // barriers, counters and twiddles ready
     for (int k = g; k < nloc; k += NG) {
         const int bf = k % NB, pl = plane_of(k), f0 = pl >> 6, f1 = pl & 63;
@@ -702,6 +731,11 @@ k_r4ring(const __grid_constant__ CUtensorMap src_map, C* __restrict__ dst, const
         pass<C, true>(v);
         twiddle<C, true>(v, tw, ac, ar);
         group_sync(g);                                 // the landed plane has been read
+        if (TS && t == 0 && pend >= 0) {
+            bulk_wait_read();                          // the previous plane's store has left its buffer
+            refill(pend);
+            pend = -1;
+        }
         put(s, L1, v);
         group_sync(g);
         get(s, L2, v);
@@ -737,17 +771,23 @@ k_r4ring(const __grid_constant__ CUtensorMap src_map, C* __restrict__ dst, const
         put(s, L2, v);
         group_sync(g);
         get(s, L1, v);
-        group_sync(g);                                 // the group is done with the buffer
-        if (t == 0 && k + NB < nloc) {
-            const int pn = plane_of(k + NB);
-            fence_async_smem();
-            mbar_expect_tx(bars + bf, (uint32_t)K::PLANE);
-            tma_load_5d(s, &src_map, 0, pn & 63, pn >> 6, 0, 0, bars + bf);
-            issued[bf] += 1;
-        }
+        group_sync(g);                                 // the group's last exchange has been read
+        if (!TS && t == 0) refill(k);
         pass<C, false>(v);
-        // ---- store: point (r, c) = (ar + 16 i, ac + 16 j), one IL-th of each sector
-        {
+        if (TS) {
+            // ---- stage the plane as [r][c] and store it with one tensor copy
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) s[(ar + 16 * i) * 64 + ac + 16 * j] = v[4 * i + j];
+            fence_async_smem();                        // generic-proxy writes visible to the tensor store
+            group_sync(g);
+            if (t == 0) {
+                tma_store_5d(&dst_map, 0, f1 % IL, 0, 0, f0 * NQ + f1 / IL, s);
+                pend = k;
+            }
+        } else {
+            // ---- store: point (r, c) = (ar + 16 i, ac + 16 j), one IL-th of each sector
             C* gd = dst + (((long long)f0 * NQ + f1 / IL) * 64 * 64 + ar * 64 + ac) * IL + (f1 % IL);
 #pragma unroll
             for (int i = 0; i < 4; ++i)
@@ -790,6 +830,13 @@ k_r4ring(const __grid_constant__ CUtensorMap src_map, C* __restrict__ dst, const
                 partials[(long long)pl * NPART + t] = tot;
             }
         }
+    }
+    if (TS && t == 0) {
+        if (pend >= 0) {
+            bulk_wait_read();
+            if (!*abort_word) refill(pend);            // another group may still need that plane
+        }
+        bulk_wait_all();                               // every store of this group has completed
     }
     __syncthreads();
     if (tid == 0 && *abort_word) {

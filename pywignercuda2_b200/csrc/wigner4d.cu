@@ -751,6 +751,7 @@ struct wig4d_plan {
     bool r4t_ready;                // k_r4t's tensor map and attributes are set
     bool r4ring;                   // complex128 64^4 Run(): persistent k_r4ring (TMA plane ring)
     bool r4ring_ready;             // k_r4ring's tensor map and attributes are set
+    bool r4ring_ts;                // k_r4ring with TMA tensor stores
     bool r4_mixed;                 // complex64 64^4: k_r4 with FP64 transforms on complex64 storage
     void* tw64d;                   // its FP64 twiddle table
     int dense_n;                   // > 0: general-delta half-steps fused (k_dense_half, N^4 grids)
@@ -762,6 +763,8 @@ struct wig4d_plan {
     void* tc_pv;                   // k_tc64's FP64 per-plane factor vectors (unshifted frequencies)
     CUtensorMap map_t_load;        // LA view of the ping-pong buffer (kinetic source)
     CUtensorMap map_w_load;        // LB view of the caller's state (potential source)
+    CUtensorMap map_t_store;       // k_r4ring stores: the ping-pong buffer (potential destination, LA)
+    CUtensorMap map_w_store;       // k_r4ring stores: the caller's state (kinetic destination, LB)
     const void* map_w_ptr;                 // state the W maps describe
     // CUDA graph of one Run() iteration, cached per (W, history, stream)
     cudaGraphExec_t graph;
@@ -1044,11 +1047,37 @@ static int encode_plane_map(CUtensorMap* m, const void* base) {
     return WIG_OK;
 }
 
-// LB map of the caller's state W (the potential half-step's source).
+// Destination view of a 64^4 complex128 array in the LA / LB layouts for the
+// tensor stores of k_r4ring: (2 float64 = 1 point, f1 % 2, c, r, unit) with
+// strides 16 B, 32 B, 2 KB, 128 KB (unit = f0 * 32 + f1 / 2); the box is one
+// plane, written into every other 16-byte slot of 64 x 64 sectors.
+static int encode_store_map(CUtensorMap* m, const void* base) {
+    const cuuint64_t dims[5] = {2, 2, 64, 64, 2048};
+    const cuuint64_t strides[4] = {16, 32, 2048, 128 * 1024};
+    const cuuint32_t box[5] = {2, 1, 64, 64, 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    EncodeTiledFn enc = encode_tiled_fn();
+    if (!enc) {
+        snprintf(wig_last_error_buffer(), 256, "cuTensorMapEncodeTiled is not available from the driver");
+        return WIG_ERR_CUDA;
+    }
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<void*>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(wig_last_error_buffer(), 256, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return WIG_ERR_CUDA;
+    }
+    return WIG_OK;
+}
+
+// LB maps of the caller's state W (the potential half-step's source, the
+// kinetic half-step's destination).
 static int ensure_w_maps(wig4d_plan* p, const void* W) {
     if (p->map_w_ptr == W) return WIG_OK;
     int s;
     if ((s = encode_plane_map(&p->map_w_load, W))) return s;
+    if ((s = encode_store_map(&p->map_w_store, W))) return s;
     p->map_w_ptr = W;
     return WIG_OK;
 }
@@ -1070,9 +1099,12 @@ static int ensure_r4ring(wig4d_plan* p) {
     if (p->r4ring_ready) return WIG_OK;
     int r;
     if ((r = ensure_r4t(p))) return r;
+    if ((r = encode_store_map(&p->map_t_store, p->pingpong))) return r;
     const int sm = (int)r4ring::Cfg<double2>::SMEM;
-    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     p->r4ring_ready = true;
     return WIG_OK;
 }
@@ -1269,22 +1301,25 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             cudaFree(t64);
             if (!ok) { wig_set_cuda_error(cudaGetLastError(), "plane vectors"); free_plan(p); return WIG_ERR_CUDA; }
         }
-        // k_r4 with cluster stores (default); WIG_FAST64_KERNEL = r4 (plain
-        // stores), r4t (complex128 TMA plane loads) or r4ring (complex128
-        // persistent TMA ring)
-        const char* kern = getenv("WIG_FAST64_KERNEL");
+        // complex128: k_r4ring with TMA tensor stores (default); complex64:
+        // k_r4 with cluster stores.  WIG_FAST64_KERNEL overrides: r4 (k_r4,
+        // plain stores), r4cluster (k_r4, cluster stores), and for complex128
+        // r4t (TMA plane loads), r4ring (ring, per-thread stores), r4ring_ts
+        const char* env_kern = getenv("WIG_FAST64_KERNEL");
+        const char* kern = env_kern ? env_kern : (desc->dtype == WIG_C128 ? "r4ring_ts" : "r4cluster");
         p->r4 = true;
-        if (desc->dtype == WIG_C128 && kern && strcmp(kern, "r4t") == 0) {
+        if (desc->dtype == WIG_C128 && strcmp(kern, "r4t") == 0) {
             int r;
             if ((r = ensure_r4t(p))) { free_plan(p); return r; }
             p->r4t = true;
         }
-        if (desc->dtype == WIG_C128 && kern && strcmp(kern, "r4ring") == 0) {
+        if (desc->dtype == WIG_C128 && (strcmp(kern, "r4ring") == 0 || strcmp(kern, "r4ring_ts") == 0)) {
             int r;
             if ((r = ensure_r4ring(p))) { free_plan(p); return r; }
             p->r4ring = true;
+            p->r4ring_ts = strcmp(kern, "r4ring_ts") == 0;
         }
-        p->r4_cluster = !(kern && strcmp(kern, "r4") == 0);
+        p->r4_cluster = strcmp(kern, "r4") != 0;
         if (cudaMalloc(&p->tw64, 64 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
         if (cudaMalloc(&p->fold, FOLD_BLOCKS * NSUM * sizeof(double)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
         if (desc->dtype == WIG_C128) k_make_r4_twiddles<double2><<<1, 64>>>((double2*)p->tw64);
@@ -1386,7 +1421,7 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     if (!p || !info) return WIG_ERR_INVALID_ARG;
     info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64;
-    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? 7 : (p->r4ring ? 8 : (p->r4t ? 4 : 3))));
+    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? 7 : (p->r4ring ? (p->r4ring_ts ? 9 : 8) : (p->r4t ? 4 : 3))));
     return WIG_OK;
 }
 
@@ -1708,15 +1743,25 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
             typedef r4ring::Cfg<double2> K;
             const unsigned grid = (unsigned)(wig_num_sms() < 4096 / K::IL ? wig_num_sms() : 4096 / K::IL);
             // kinetic: LA (ping-pong) -> LB (W); potential: LB (W) -> LA (ping-pong)
+            const double2* tw = (const double2*)p->tw64;
+            const double2* pvp = pv + (size_t)p->shape[0] * p->shape[2] * 128;
+            double2* P = reinterpret_cast<double2*>(p->pingpong);
+            const double2 ks = make_double2(p->kin_scale, 0.0), ps = make_double2(p->pot_scale, 0.0);
             if (part == 0) {
-                k_r4ring<double2, true><<<grid, K::NTH, K::SMEM, st>>>(p->map_t_load, W, pv, (const double2*)p->tw64,
-                                                                       make_double2(p->kin_scale, 0.0), p->cur_norm,
-                                                                       p->ob, nullptr);
+                if (p->r4ring_ts)
+                    k_r4ring<double2, true, true><<<grid, K::NTH, K::SMEM, st>>>(p->map_t_load, p->map_w_store, W, pv,
+                                                                                 tw, ks, p->cur_norm, p->ob, nullptr);
+                else
+                    k_r4ring<double2, true, false><<<grid, K::NTH, K::SMEM, st>>>(p->map_t_load, p->map_w_store, W, pv,
+                                                                                  tw, ks, p->cur_norm, p->ob, nullptr);
                 WIG_LAUNCHED("k_r4ring<kin>");
             } else if (part == 1) {
-                k_r4ring<double2, false><<<grid, K::NTH, K::SMEM, st>>>(
-                    p->map_w_load, reinterpret_cast<double2*>(p->pingpong), pv + (size_t)p->shape[0] * p->shape[2] * 128,
-                    (const double2*)p->tw64, make_double2(p->pot_scale, 0.0), p->cur_norm, p->ob, p->partials);
+                if (p->r4ring_ts)
+                    k_r4ring<double2, false, true><<<grid, K::NTH, K::SMEM, st>>>(p->map_w_load, p->map_t_store, P, pvp,
+                                                                                  tw, ps, p->cur_norm, p->ob, p->partials);
+                else
+                    k_r4ring<double2, false, false><<<grid, K::NTH, K::SMEM, st>>>(p->map_w_load, p->map_t_store, P, pvp,
+                                                                                   tw, ps, p->cur_norm, p->ob, p->partials);
                 WIG_LAUNCHED("k_r4ring<pot>");
             } else {
                 return fold_and_finalize(p, hist, rows, st);
@@ -1905,20 +1950,22 @@ struct TuneKey {
 struct TuneChoice { int engine, kin48, pot_gmax; };
 
 // engine: 0 k_r4 plain stores, 1 k_r4 cluster stores, 2 k_r4t, 3 k_tc64,
-// 4 the CUDA-core path of a plan without the 64^4 radix kernels, 5 k_r4ring
+// 4 the CUDA-core path of a plan without the 64^4 radix kernels, 5 k_r4ring,
+// 6 k_r4ring with TMA tensor stores
 int apply_choice(wig4d_plan* p, const TuneChoice& c) {
     if (c.engine == 2) {
         const int r = ensure_r4t(p);
         if (r) return r;
     }
-    if (c.engine == 5) {
+    if (c.engine == 5 || c.engine == 6) {
         const int r = ensure_r4ring(p);
         if (r) return r;
     }
     p->tc = c.engine == 3;
     p->r4_cluster = c.engine == 1;
     p->r4t = c.engine == 2;
-    p->r4ring = c.engine == 5;
+    p->r4ring = c.engine == 5 || c.engine == 6;
+    p->r4ring_ts = c.engine == 6;
     p->kin48 = c.kin48 != 0;
     p->pot_gmax = c.pot_gmax;
     if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
@@ -1927,7 +1974,7 @@ int apply_choice(wig4d_plan* p, const TuneChoice& c) {
 
 TuneChoice current_choice(const wig4d_plan* p) {
     TuneChoice c;
-    c.engine = p->tc ? 3 : (p->r4 ? (p->r4ring ? 5 : (p->r4t ? 2 : (p->r4_cluster ? 1 : 0))) : 4);
+    c.engine = p->tc ? 3 : (p->r4 ? (p->r4ring ? (p->r4ring_ts ? 6 : 5) : (p->r4t ? 2 : (p->r4_cluster ? 1 : 0))) : 4);
     c.kin48 = p->kin48;
     c.pot_gmax = p->pot_gmax;
     return c;
@@ -1966,6 +2013,7 @@ extern "C" int wig4d_autotune(wig4d_plan* p, int iterations, int flags, void* st
         engines.push_back({0, base.kin48, base.pot_gmax});
         if (p->dtype == WIG_C128) engines.push_back({2, base.kin48, base.pot_gmax});
         if (p->dtype == WIG_C128) engines.push_back({5, base.kin48, base.pot_gmax});
+        if (p->dtype == WIG_C128) engines.push_back({6, base.kin48, base.pot_gmax});
     } else {
         engines.push_back({4, base.kin48, base.pot_gmax});
     }
