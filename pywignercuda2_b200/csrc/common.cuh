@@ -87,3 +87,23 @@ __device__ __forceinline__ void cp_async_elem(float2* dst, const float2* src) {
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// ---------------------------------------------------------------------------
+// Epilogue of the Wigner-Dirac Theta -> P plane transform on 64^4 grids that
+// also runs the next Run() iteration's first three passes: boundary_xp (the
+// product of the four per-axis factors), Real_GPU of the diagonal components
+// and the observable sums of the result.  Each plane writes one row of
+// DEPI_SUMS partial sums (the layout of the Dirac reductions:
+// 0,1 trace, 2..9 x/p_x/y/p_y moments of the trace, 10,11 alpha, 12,13 x
+// alpha1 / y alpha2, 14 kinetic, 15 potential energy, 16..18 D1A0..D1A2).
+// ---------------------------------------------------------------------------
+#define DEPI_SUMS 20
+struct DEpi {
+    const double* mxp[4];                   // boundary_xp factors per axis (i0 .. i3)
+    const double* cx; const double* cy;     // x[N_x], y[N_y]
+    const double* cpx; const double* cpy;   // p_x[N_px], p_y[N_py]
+    const double* obs_xy;                   // [7][N_y][N_x]: A0, A1, A2, A3, D1A0, D1A1, D1A2
+    double c, mass;
+    int kvn;
+    double* rows;                           // [slot][i1 * 64 + i3][DEPI_SUMS]
+};

@@ -27,7 +27,7 @@
 void* wig_dense_matrix(int n, double delta, int dtype, cudaStream_t st);
 int wig_r4_twiddles(void* tw, int dtype, cudaStream_t st);
 int wig_dplane64(void* const* slots, int nslots, int dtype, int kind, int fwd, double scale, const double* d_norm,
-                 const void* tw, cudaStream_t st);
+                 const void* tw, cudaStream_t st, const DEpi* epi = nullptr);
 
 #define NSLOT 16
 
@@ -542,6 +542,21 @@ __global__ void __launch_bounds__(256, 2) k_dmask_real_reduce(Slots<C> S, DParam
     dreduce_block(a, partials);
 }
 
+// The fused Theta -> P epilogue's per-plane rows -> EPI_FOLD rows: block b
+// adds its contiguous share of the rows, one warp per column (a fixed order).
+#define EPI_FOLD 256
+static_assert(DSUM == DEPI_SUMS, "the epilogue rows have the layout of the reductions");
+__global__ void k_dfold(const double* __restrict__ rows, int nrows, double* __restrict__ out) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int per = (nrows + gridDim.x - 1) / gridDim.x, r0 = blockIdx.x * per;
+    const int r1 = r0 + per < nrows ? r0 + per : nrows;
+    double t = 0.0;
+    for (int r = r0 + l; r < r1; r += 32) t += rows[(long long)r * DSUM + w];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (l == 0) out[(long long)blockIdx.x * DSUM + w] = t;
+}
+
 // out: [norm_re, norm_im, 17 observables] = WIGD_NOBS values.  When divide,
 // observables are divided by the trace norm as Run() sees them after
 // Normalize (the real part of 1/norm: the sums are of real parts); else they
@@ -694,6 +709,8 @@ struct wigd_plan {
     int nblk;
     void* tw64;              // twiddles of k_dplane_r4 (64^4 grids only)
     double* afull;           // full A1..A3 tables (fields that are not of low rank)
+    double* epi_rows;        // 64^4: per-plane sums of the fused Theta -> P epilogue [16][4096][DSUM]
+    double* epi_fold;        // and their EPI_FOLD folded rows
 };
 
 static unsigned dgrid(long long n, int threads = 256, int per_sm = 8) {
@@ -708,6 +725,8 @@ static void free_dplan(wigd_plan* p) {
     cudaFree(p->partials);
     cudaFree(p->cur_norm);
     cudaFree(p->tw64);
+    cudaFree(p->epi_rows);
+    cudaFree(p->epi_fold);
     cudaFree(p->afull);
     delete p;
 }
@@ -837,6 +856,10 @@ extern "C" int wigd_plan_create(const wigd_desc* desc, wigd_plan** out) {
     if (N0 == 64 && N1 == 64 && N2 == 64 && N3 == 64) {
         if (cudaMalloc(&p->tw64, 64 * sizeof(double2)) != cudaSuccess) { free_dplan(p); return WIG_ERR_ALLOC; }
         if (wig_r4_twiddles(p->tw64, desc->dtype, 0) != WIG_OK) { free_dplan(p); return WIG_ERR_CUDA; }
+        if (cudaMalloc(&p->epi_rows, (size_t)NSLOT * 4096 * DSUM * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&p->epi_fold, (size_t)EPI_FOLD * DSUM * sizeof(double)) != cudaSuccess) {
+            free_dplan(p); return WIG_ERR_ALLOC;
+        }
     }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { wig_set_cuda_error(e, "wigd_plan_create"); free_dplan(p); return WIG_ERR_CUDA; }
@@ -1027,7 +1050,8 @@ extern "C" int wigd_init_landau(wigd_plan* p, void* const* slots, double B, doub
 #define DPLANE_CASES(X) X(16, 16) X(32, 32) X(64, 64) X(128, 128) X(64, 128) X(128, 64)
 
 template <class C, int KIND, bool FWD>
-static int launch_dplane(wigd_plan* p, const Slots<C>& S, int nslots, double2 sc, const double* d_norm, cudaStream_t st) {
+static int launch_dplane(wigd_plan* p, const Slots<C>& S, int nslots, double2 sc, const double* d_norm, cudaStream_t st,
+                         const DEpi* epi = nullptr) {
     const int NA = KIND == 0 ? p->d.shape[1] : p->d.shape[0];
     const int NB = KIND == 0 ? p->d.shape[3] : p->d.shape[2];
     const unsigned planes = KIND == 0 ? (unsigned)(p->d.shape[0] * p->d.shape[2]) : (unsigned)(p->d.shape[1] * p->d.shape[3]);
@@ -1035,8 +1059,9 @@ static int launch_dplane(wigd_plan* p, const Slots<C>& S, int nslots, double2 sc
     if (p->tw64 && !getenv("WIG_NO_DPLANE_R4")) {   // 64^4: radix-4 register transform
         void* ptrs[NSLOT];
         for (int k = 0; k < nslots; ++k) ptrs[k] = S.p[k];
-        return wig_dplane64(ptrs, nslots, p->d.dtype, KIND, FWD ? 1 : 0, sc.x, d_norm, p->tw64, st);
+        return wig_dplane64(ptrs, nslots, p->d.dtype, KIND, FWD ? 1 : 0, sc.x, d_norm, p->tw64, st, epi);
     }
+    if (epi) return WIG_ERR_UNSUPPORTED;
     constexpr int G = 32 / (int)sizeof(C);
 #define DCASE(a, b)                                                                              \
     if (NA == a && NB == b) {                                                                    \
@@ -1067,7 +1092,8 @@ static int launch_dplane(wigd_plan* p, const Slots<C>& S, int nslots, double2 sc
 
 // which: 0 X->Lambda, 1 Lambda->X, 2 P->Theta, 3 Theta->P.
 template <class C>
-static int transform_impl(wigd_plan* p, void* const* slots, int nslots, int which, const double* d_norm, cudaStream_t st) {
+static int transform_impl(wigd_plan* p, void* const* slots, int nslots, int which, const double* d_norm, cudaStream_t st,
+                          const DEpi* epi = nullptr) {
     if (nslots < 1 || nslots > NSLOT) return WIG_ERR_INVALID_ARG;
     Slots<C> S;
     for (int k = 0; k < NSLOT; ++k) S.p[k] = nullptr;
@@ -1092,9 +1118,10 @@ static int transform_impl(wigd_plan* p, void* const* slots, int nslots, int whic
         if (kind == 0) r = sgn > 0 ? launch_dplane<C, 0, true>(p, S, nslots, make_double2(sc, 0.0), d_norm, st)
                                    : launch_dplane<C, 0, false>(p, S, nslots, make_double2(sc, 0.0), d_norm, st);
         else r = sgn > 0 ? launch_dplane<C, 1, true>(p, S, nslots, make_double2(sc, 0.0), d_norm, st)
-                         : launch_dplane<C, 1, false>(p, S, nslots, make_double2(sc, 0.0), d_norm, st);
-        if (r != WIG_ERR_UNSUPPORTED) return r;
+                         : launch_dplane<C, 1, false>(p, S, nslots, make_double2(sc, 0.0), d_norm, st, epi);
+        if (r != WIG_ERR_UNSUPPORTED || epi) return r;
     }
+    if (epi) return WIG_ERR_UNSUPPORTED;
     // general delta or size: two standalone FAFTs per slot (in slot order)
     for (int k = 0; k < nslots; ++k) {
         int r = wig_faft(slots[k], ns, p->d.dtype, ax_b, p->d.d[ax_b], sgn * p->d.delta[ax_b], 1.0, st);
@@ -1121,10 +1148,27 @@ static int run_impl(wigd_plan* p, void* const* slots, int iterations, int filter
     Slots<C> S;
     if ((r = make_slots(slots, S, false))) return r;
     const bool fused_mrr = getenv("WIG_NO_DFUSE") == nullptr;
+    // 64^4 with |delta| N = 1 on the P <-> Theta axes: the Theta -> P transform
+    // of iteration it also runs iteration it + 1's boundary_xp, Real and sums
+    auto fast = [&](int a) { return fabs(fabs(p->d.delta[a]) * p->d.shape[a] - 1.0) < 1e-12; };
+    const bool fuse_tp = fused_mrr && p->epi_rows && fast(0) && fast(2) && !getenv("WIG_NO_DTP_FUSE") &&
+                         !getenv("WIG_NO_DPLANE_R4") && !getenv("WIG_NO_DPLANE_TMA");
+    DEpi E;
+    memset(&E, 0, sizeof(E));
+    for (int a = 0; a < 4; ++a) E.mxp[a] = p->P.mxp[a];
+    E.cx = p->P.cx; E.cy = p->P.cy; E.cpx = p->P.cpx; E.cpy = p->P.cpy;
+    E.obs_xy = p->P.obs_xy; E.c = p->P.c; E.mass = p->P.mass; E.kvn = p->P.kvn; E.rows = p->epi_rows;
     WIG_CUDA(cudaMemsetAsync(p->counter, 0, 2 * sizeof(int), st));
     for (int it = 0; it < iterations; ++it) {
         // boundary_xp, Real, trace norm + observables of the normalised state
-        if (fused_mrr) {
+        if (fuse_tp && it > 0) {
+            // done by the previous Theta -> P: fold its per-plane sums
+            k_dfold<<<EPI_FOLD, 32 * DSUM, 0, st>>>(p->epi_rows, NSLOT * 4096, p->epi_fold);
+            WIG_LAUNCHED("k_dfold");
+            k_dfinalize<<<1, 32 * DSUM, 0, st>>>(p->epi_fold, EPI_FOLD, p->d.dv_norm, p->d.dv_obs, 1, hist,
+                                                 p->counter, iterations, p->cur_norm, p->flag);
+            WIG_LAUNCHED("k_dfinalize");
+        } else if (fused_mrr) {
             k_dmask_real_reduce<C><<<p->nblk, 256, 0, st>>>(S, p->P, p->partials);
             WIG_LAUNCHED("k_dmask_real_reduce");
             k_dfinalize<<<1, 32 * DSUM, 0, st>>>(p->partials, p->nblk, p->d.dv_norm, p->d.dv_obs, 1, hist,
@@ -1141,7 +1185,8 @@ static int run_impl(wigd_plan* p, void* const* slots, int iterations, int filter
         if ((r = transform_impl<C>(p, slots, NSLOT, 1, nullptr, st))) return r;
         if ((r = transform_impl<C>(p, slots, NSLOT, 2, nullptr, st))) return r;
         if ((r = potential_impl<C>(p, slots, st))) return r;
-        if ((r = transform_impl<C>(p, slots, NSLOT, 3, nullptr, st))) return r;
+        if ((r = transform_impl<C>(p, slots, NSLOT, 3, nullptr, st, fuse_tp && it + 1 < iterations ? &E : nullptr)))
+            return r;
     }
     return WIG_OK;
 }

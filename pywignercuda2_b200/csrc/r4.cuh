@@ -957,12 +957,65 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, int c0, int
 template <class C>
 constexpr int dplane_gp() { return 16 / (int)sizeof(C); }
 template <class C>
-constexpr size_t dplane_r4t_smem_bytes() { return 128 + 65536 + 64 * sizeof(C) + 16; }
+constexpr size_t dplane_r4t_smem_bytes() { return 128 + 65536 + 64 * sizeof(C) + 16 + 2 * 8 * 8 * sizeof(double); }
 
-template <class C, bool FWD>
+// EPI (Theta -> P only): boundary_xp and Real_GPU of the diagonal on the
+// transformed values before they are stored (the same rounding as the
+// separate passes: the stored transform value, scaled in FP64 by the
+// product of the four factors in the order k_dmask_real_reduce uses), and
+// one row of DEPI_SUMS sums per plane of the stored result.  In a plane
+// (i1, i3) only p_x = cpx[i2] and p_y = cpy[i0] vary, so each thread keeps
+// seven moments (sum Re w * {1, p_x, p_x^2, p_y, p_y^2}, sum Im w * {1, p_y});
+// one thread per plane turns the plane's moments into its component's share
+// of the sums (depi_row).
+namespace depi {
+constexpr int NM = 7;
+// the 20 sums of one component k from its plane's moments m at (x, y) with
+// the field tables of the plane (A0..A3, D1A0..D1A2)
+__device__ __forceinline__ void row(const DEpi& E, int k, double x, double y, const double (&A)[7],
+                                    const double (&m)[NM], double* out) {
+    double a[DEPI_SUMS];
+#pragma unroll
+    for (int q = 0; q < DEPI_SUMS; ++q) a[q] = 0.0;
+    const double R0 = m[0], Rpx = m[1], Rpx2 = m[2], Rpy = m[3], Rpy2 = m[4], I0 = m[5], Ipy = m[6];
+    const double c = E.c;
+    if (k == 0 || k == 5 || k == 10 || k == 15) {          // the trace W11 + W22 + W33 + W44
+        const double sg = k < 10 ? 1.0 : -1.0;             // mass term Re(W11 + W22 - W33 - W44)
+        a[0] = R0; a[1] = I0;
+        a[2] = x * R0; a[3] = Rpx; a[4] = x * x * R0; a[5] = Rpx2;
+        a[6] = y * R0; a[7] = Rpy; a[8] = y * y * R0; a[9] = Rpy2;
+        a[14] = sg * E.mass * c * c * R0;
+        a[15] = c * A[0] * R0;
+        a[16] = c * A[4] * R0;
+    } else if (k == 3 || k == 12 || k == 6 || k == 9) {    // W14, W41, W23, W32
+        // alpha1 = Re(W14 + W41 + W23 + W32); alpha2 = -Im(W14 - W41 + W32 - W23)
+        const double tau = (k == 3 || k == 9) ? -1.0 : 1.0;
+        a[10] = R0; a[12] = x * R0;
+        a[11] = tau * I0; a[13] = tau * y * I0;
+        a[14] = c * Rpx + tau * c * Ipy;
+        a[17] = c * A[5] * R0;
+        if (E.kvn) {   // k2 = Im(W14 - W41 - W23 + W32), and Re of the same combination
+            const double kap = (k == 3 || k == 9) ? 1.0 : -1.0;
+            a[15] = A[1] * c * R0 - A[2] * c * kap * I0;
+            a[18] = c * A[6] * kap * R0;
+        } else {       // e2 = Im(-W14 + W23 - W32 + W41) = alpha2
+            a[15] = -A[1] * c * R0 - A[2] * c * tau * I0;
+            a[18] = -A[6] * c * tau * I0;
+        }
+    } else if (!E.kvn && (k == 2 || k == 7 || k == 8 || k == 13)) {   // e3 = Re(-W13 + W24 - W31 + W42)
+        const double eps = (k == 2 || k == 8) ? -1.0 : 1.0;
+        a[15] = A[3] * c * eps * R0;
+    }
+#pragma unroll
+    for (int q = 0; q < DEPI_SUMS; ++q) out[q] = a[q];
+}
+}  // namespace depi
+
+template <class C, bool FWD, bool EPI = false>
 __global__ void __launch_bounds__(r4::NT * dplane_gp<C>(), 2)
-k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, PlaneSlots<C> S, const C* __restrict__ gtw, double2 scale,
-             const double* __restrict__ d_norm) {
+k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, const __grid_constant__ PlaneSlots<C> S,
+             const C* __restrict__ gtw, double2 scale, const double* __restrict__ d_norm,
+             const __grid_constant__ DEpi E) {
     using namespace r4;
     constexpr int GP = dplane_gp<C>();
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -1018,12 +1071,67 @@ k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, PlaneSlots<C> S, const C
     const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
     const C ccs = ((r2 + c2) & 1) ? cneg(cc) : cc;
     __syncthreads();                                   // every group's last exchange has been read
+    if (!EPI) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-            s[((r2 + 4 * r1 + 16 * i) * 64 + c2 + 4 * c1 + 16 * j) * GP + grp] = cmul(v[4 * i + j], ccs);
+            for (int j = 0; j < 4; ++j)
+                s[((r2 + 4 * r1 + 16 * i) * 64 + c2 + 4 * c1 + 16 * j) * GP + grp] = cmul(v[4 * i + j], ccs);
+    } else {
+        // output point (i0, i2) = (r2 + 4 r1 + 16 i, c2 + 4 c1 + 16 j) of plane (i1, i3)
+        const int slot = blockIdx.y, i3 = GP * m + grp;
+        const bool diag = slot == 0 || slot == 5 || slot == 10 || slot == 15;
+        const double m13 = E.mxp[3][i3], m11 = E.mxp[1][i1];
+        double mo[depi::NM];
+#pragma unroll
+        for (int q = 0; q < depi::NM; ++q) mo[q] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int i0 = r2 + 4 * r1 + 16 * i;
+            const double m0 = E.mxp[0][i0], py = E.cpy[i0];
+            double sr = 0.0, sx = 0.0, sx2 = 0.0, si = 0.0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int i2 = c2 + 4 * c1 + 16 * j;
+                const double r = E.mxp[2][i2] * m0 * m13 * m11;
+                const double2 d = to_d2(cmul(v[4 * i + j], ccs));   // the value a plain transform stores
+                C w = to_c<C>(make_double2(d.x * r, d.y * r));
+                if (diag) w.y = 0;
+                s[(i0 * 64 + i2) * GP + grp] = w;
+                const double px = E.cpx[i2], wr = (double)w.x, wi = (double)w.y;
+                sr += wr; sx = fma(px, wr, sx); sx2 = fma(px * px, wr, sx2); si += wi;
+            }
+            mo[0] += sr; mo[1] += sx; mo[2] += sx2;
+            mo[3] = fma(py, sr, mo[3]); mo[4] = fma(py * py, sr, mo[4]);
+            mo[5] += si; mo[6] = fma(py, si, mo[6]);
+        }
+        // plane sums: warps, then the group's 8 warps in shared memory
+#pragma unroll
+        for (int q = 0; q < depi::NM; ++q)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mo[q] += __shfl_down_sync(0xffffffffu, mo[q], o);
+        double* red = reinterpret_cast<double*>(bar + 2) + grp * 64;
+        const int w = t >> 5, l = t & 31;
+        if (l == 0)
+#pragma unroll
+            for (int q = 0; q < depi::NM; ++q) red[w * 8 + q] = mo[q];
+        __syncthreads();
+        if (t == 0) {
+            double tot[depi::NM];
+#pragma unroll
+            for (int q = 0; q < depi::NM; ++q) {
+                tot[q] = 0.0;
+                for (int ww = 0; ww < 8; ++ww) tot[q] += red[ww * 8 + q];
+            }
+            const long long ixy = (long long)i1 * 64 + i3;
+            double A[7];
+#pragma unroll
+            for (int q = 0; q < 7; ++q) A[q] = E.obs_xy[q * 4096 + ixy];
+            depi::row(E, slot, E.cx[i3], E.cy[i1], A, tot, E.rows + ((long long)slot * 4096 + ixy) * DEPI_SUMS);
+        }
+    }
     r4t::fence_async_smem();                           // generic-proxy writes visible to the tensor store
     __syncthreads();
     if (threadIdx.x == 0) dpt::tma_store_4d(map, 2 * GP * m, 0, i1, 0, s);
 }
+

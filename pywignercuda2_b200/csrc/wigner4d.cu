@@ -1475,7 +1475,7 @@ static int encode_dplane_map(CUtensorMap* m, const void* base, int reals, int ro
 
 template <class C, bool FWD>
 static int launch_dplane_r4t(void* const* slots, int nslots, const void* tw, double scale, const double* d_norm,
-                             cudaStream_t st) {
+                             cudaStream_t st, const DEpi* epi = nullptr) {
     PlaneMaps<C> maps;
     PlaneSlots<C> S;
     memset(&maps, 0, sizeof(maps));
@@ -1485,26 +1485,43 @@ static int launch_dplane_r4t(void* const* slots, int nslots, const void* tw, dou
         if ((r = encode_dplane_map<C>(&maps.m[k], slots[k], 2 * dplane_gp<C>(), 64))) return r;
     }
     constexpr int GP = dplane_gp<C>();
-    auto kern = k_dplane_r4t<C, FWD>;
     const size_t sm = dplane_r4t_smem_bytes<C>();
+    if constexpr (!FWD) {
+        if (epi) {
+            if (nslots != 16) return WIG_ERR_INVALID_ARG;
+            auto kern = k_dplane_r4t<C, FWD, true>;
+            WIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            kern<<<dim3(64 * 64 / GP, nslots), r4::NT * GP, sm, st>>>(maps, S, (const C*)tw,
+                                                                      make_double2(scale, 0.0), d_norm, *epi);
+            WIG_LAUNCHED("k_dplane_r4t<epi>");
+            return WIG_OK;
+        }
+    }
+    if (epi) return WIG_ERR_INVALID_ARG;
+    auto kern = k_dplane_r4t<C, FWD, false>;
     WIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    DEpi none;
+    memset(&none, 0, sizeof(none));
     kern<<<dim3(64 * 64 / GP, nslots), r4::NT * GP, sm, st>>>(maps, S, (const C*)tw, make_double2(scale, 0.0),
-                                                              d_norm);
+                                                              d_norm, none);
     WIG_LAUNCHED("k_dplane_r4t");
     return WIG_OK;
 }
 
 // kind 0: axes (1, 3), kind 1: axes (0, 2) of a 64^4 component; fwd: exp(-i ...)
+// epi (Theta -> P, kind 1, fwd 0, all 16 slots): fuse the next iteration's
+// boundary_xp, Real and sums into the transform (k_dplane_r4t<EPI>)
 int wig_dplane64(void* const* slots, int nslots, int dtype, int kind, int fwd, double scale, const double* d_norm,
-                 const void* tw, cudaStream_t st) {
+                 const void* tw, cudaStream_t st, const DEpi* epi) {
     if (nslots < 1 || nslots > 16 || !tw) return WIG_ERR_INVALID_ARG;
     for (int k = 0; k < nslots; ++k)
         if (!slots[k] || (reinterpret_cast<uintptr_t>(slots[k]) & 15)) return WIG_ERR_INVALID_ARG;
+    if (epi && (kind != 1 || fwd || getenv("WIG_NO_DPLANE_TMA"))) return WIG_ERR_UNSUPPORTED;
     if (kind == 1 && !getenv("WIG_NO_DPLANE_TMA")) {
         if (dtype == WIG_C128) return fwd ? launch_dplane_r4t<double2, true>(slots, nslots, tw, scale, d_norm, st)
-                                          : launch_dplane_r4t<double2, false>(slots, nslots, tw, scale, d_norm, st);
+                                          : launch_dplane_r4t<double2, false>(slots, nslots, tw, scale, d_norm, st, epi);
         return fwd ? launch_dplane_r4t<float2, true>(slots, nslots, tw, scale, d_norm, st)
-                   : launch_dplane_r4t<float2, false>(slots, nslots, tw, scale, d_norm, st);
+                   : launch_dplane_r4t<float2, false>(slots, nslots, tw, scale, d_norm, st, epi);
     }
     if (dtype == WIG_C128) {
         if (kind == 0) return fwd ? launch_dplane_r4<double2, 0, true>(slots, nslots, tw, scale, d_norm, st)

@@ -20,7 +20,7 @@ from frames import make_frame, rel_err  # noqa: E402
 from golden.notebook_configs import NOTEBOOKS  # noqa: E402
 from oracle.dirac4d import DiracOracle  # noqa: E402
 from pywignercuda2_b200 import GPU_WignerDirac4D, GPU_WignerDiracKvN4D  # noqa: E402
-from pywignercuda2_b200.dirac4d import NAMES  # noqa: E402
+from pywignercuda2_b200.dirac4d import NAMES, OBS_NAMES  # noqa: E402
 
 GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "notebook_norms.json")))
 
@@ -287,6 +287,38 @@ def test_run_64_matches_generic_planes(monkeypatch):
         out.append((np.array(f.norms), np.array(f.energyKinetic), np.array(f.average_x), f.W11.get(), f.W14.get()))
     for a, b in zip(out[0], out[1]):
         assert rel_err(a, b) < 1e-11
+
+
+@pytest.mark.parametrize("kvn", [False, True])
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_run_64_theta_to_p_epilogue(dtype, kvn, monkeypatch):
+    """The fused loop at 64^4: the Theta -> P transform that also runs the
+    next iteration's boundary_xp, Real and sums (k_dplane_r4t<EPI>) against
+    the separate pass (WIG_NO_DTP_FUSE).  The sums are added in another
+    order, so the norm (and the next 1/norm scale) differs in the last bits:
+    sums and states agree to 1e-12 relative to their largest value (1e-6 in
+    complex64, where the scale is rounded to float32)."""
+    p = small(64, kvn, fast=True)
+    cls = GPU_WignerDiracKvN4D if kvn else GPU_WignerDirac4D
+    out = []
+    for env in (None, "1"):
+        if env:
+            monkeypatch.setenv("WIG_NO_DTP_FUSE", env)
+        f = make_frame(cls, p, alias_w21=False, bound_p=15.0, complex_dtype=dtype)
+        f.fileName = None
+        f.timeSteps = 3
+        Ws = all_w(f)
+        f.WignerDiracGaussian_ParticleUp_GPU(*Ws, 0.5, 0.1, 0.3, -0.2, 2.2, 1.9)
+        f._Fourier_Theta_To_P_64_64_4x4_GPU(*Ws)
+        f.Run()
+        out.append(([np.array(f.norms)] + [np.array(getattr(f, k)) for k in OBS_NAMES], [W.get() for W in Ws]))
+        del f
+    monkeypatch.delenv("WIG_NO_DTP_FUSE")
+    tol = 1e-12 if dtype == np.complex128 else 1e-6
+    for k, (a, b) in enumerate(zip(out[0][0], out[1][0])):
+        # observables that vanish for this state sit at ~1e-19: scale by max(|b|, 1)
+        assert np.max(np.abs(a - b)) <= tol * max(np.max(np.abs(b)), 1.0), k
+    assert err16(out[0][1], out[1][1]) < tol
 
 
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
