@@ -268,7 +268,8 @@ int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
    wig4d_desc.transform = 1), 7 k_r4 with FP64 transforms on complex64
    storage (wig4d_desc.transform = 3), 8 k_r4ring (complex128 persistent
    k_r4 with a TMA ring of planes, WIG_FAST64_KERNEL=r4ring), 9 k_r4ring
-   with TMA tensor stores (WIG_FAST64_KERNEL=r4ring_ts). */
+   with TMA tensor stores (WIG_FAST64_KERNEL=r4ring_ts), 10 k_r4ring on the
+   plane-contiguous layouts with bulk stores (the complex128 default). */
 int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
 
 
@@ -285,7 +286,7 @@ int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
  * without timing unless flags has WIG_TUNE_FORCE.  choice_out (host, 4
  * ints, may be NULL) receives the engine (0 k_r4 plain, 1 k_r4 cluster,
  * 2 k_r4t, 3 k_tc64, 4 the per-size kernels, 5 k_r4ring, 6 k_r4ring with
- * TMA stores), k_kin48 (1/0), the columns
+ * TMA stores, 7 k_r4ring on plane-contiguous layouts), k_kin48 (1/0), the columns
  * per CTA and the number of candidates timed.  Allocates a scratch state;
  * synchronous; call it outside any stream capture.
  */

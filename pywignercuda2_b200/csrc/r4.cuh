@@ -621,6 +621,14 @@ __device__ __forceinline__ void tma_store_5d(const CUtensorMap* map, int c0, int
                  : "memory");
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
+// one contiguous block from shared to global memory (bulk group of the issuing
+// thread); both addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_store_1d(void* gdst, const void* ssrc, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(r4t::sa(ssrc)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
@@ -653,7 +661,14 @@ __device__ __forceinline__ double warp_slot_sums(double (&a)[16], int lane) {
 // waits until the store has read it, which the group's thread 0 checks at
 // the group's next plane (after reading its input) or after its last plane.
 // Without TS each thread stores its 16 points (one IL-th of 16 sectors).
-template <class C, bool KIN, bool TS>
+// PC (with TS): the plane-contiguous layouts LK = [y][x][p_y][p_x] (kinetic
+// source, potential destination) and LP = [p_y][p_x][y][x] (the reverse).
+// Both half-steps then read point (r, c) of plane (f0, f1) at
+// src[((r * 64 + c) * 64 + f0) * 64 + f1] -- a box of one-point rows whose
+// sectors the other group's plane (f1 ^ 1) reads at the same time -- and
+// write the plane as one contiguous 64 KB block at dst + (f0 * 64 + f1) *
+// 4096 with a single bulk copy: whole lines, no partial-sector writes.
+template <class C, bool KIN, bool TS, bool PC = false>
 __global__ void __launch_bounds__(r4ring::Cfg<C>::NTH, 1)
 k_r4ring(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map,
          C* __restrict__ dst, const double2* __restrict__ PV, const C* __restrict__ gtw, double2 scale,
@@ -783,7 +798,8 @@ k_r4ring(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CU
             fence_async_smem();                        // generic-proxy writes visible to the tensor store
             group_sync(g);
             if (t == 0) {
-                tma_store_5d(&dst_map, 0, f1 % IL, 0, 0, f0 * NQ + f1 / IL, s);
+                if (PC) bulk_store_1d(dst + (long long)pl * 4096, s, (uint32_t)K::PLANE);
+                else tma_store_5d(&dst_map, 0, f1 % IL, 0, 0, f0 * NQ + f1 / IL, s);
                 pend = k;
             }
         } else {
@@ -843,6 +859,33 @@ k_r4ring(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CU
         // no copy may still target this CTA's shared memory when it exits
         for (int b = 0; b < NB; ++b)
             if (issued[b] > 0) wait_plane(bars + b, issued + b, issued[b] - 1, issued + NB + 1);
+    }
+}
+
+// Conversions between the reference layout [p_y][y][p_x][x] and k_r4ring's
+// LK = [y][x][p_y][p_x]: for each (p_y, y) a 64 x 64 transpose of (p_x, x)
+// through a shared tile (both sides move whole 1 KB rows).  TO: W -> LK;
+// else LK -> W divided by the complex norm (none when d_norm is null).
+// Grid (2, 2, 4096) of 32 x 8 threads; blockIdx.z = p_y * 64 + y.
+template <class C, bool TO>
+__global__ void __launch_bounds__(256) k_pc_transpose(const C* __restrict__ src, C* __restrict__ dst,
+                                                      const double* __restrict__ d_norm) {
+    __shared__ C tile[32][33];
+    const int py = blockIdx.z >> 6, y = blockIdx.z & 63;
+    // u: the source's contiguous index, v: the destination's
+    const long long sbase = TO ? ((long long)py * 64 + y) * 4096 : (long long)y * 262144 + py * 64;
+    const long long dbase = TO ? (long long)y * 262144 + py * 64 : ((long long)py * 64 + y) * 4096;
+    const long long sstride = TO ? 64 : 4096, dstride = TO ? 4096 : 64;
+    const int u0 = blockIdx.x * 32, v0 = blockIdx.y * 32, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) tile[ty + k][tx] = src[sbase + (long long)(v0 + ty + k) * sstride + u0 + tx];
+    __syncthreads();
+    double2 inv = make_double2(1.0, 0.0);
+    if (!TO && d_norm) inv = zinv(make_double2(d_norm[0], d_norm[1]));
+#pragma unroll
+    for (int k = 0; k < 32; k += 8) {
+        const C a = tile[tx][ty + k];
+        dst[dbase + (long long)(u0 + ty + k) * dstride + v0 + tx] = TO ? a : to_c<C>(zmul(to_d2(a), inv));
     }
 }
 

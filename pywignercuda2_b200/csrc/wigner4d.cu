@@ -752,6 +752,7 @@ struct wig4d_plan {
     bool r4ring;                   // complex128 64^4 Run(): persistent k_r4ring (TMA plane ring)
     bool r4ring_ready;             // k_r4ring's tensor map and attributes are set
     bool r4ring_ts;                // k_r4ring with TMA tensor stores
+    bool r4ring_pc;                // k_r4ring on the plane-contiguous layouts LK / LP (bulk stores)
     bool r4_mixed;                 // complex64 64^4: k_r4 with FP64 transforms on complex64 storage
     void* tw64d;                   // its FP64 twiddle table
     int dense_n;                   // > 0: general-delta half-steps fused (k_dense_half, N^4 grids)
@@ -765,6 +766,8 @@ struct wig4d_plan {
     CUtensorMap map_w_load;        // LB view of the caller's state (potential source)
     CUtensorMap map_t_store;       // k_r4ring stores: the ping-pong buffer (potential destination, LA)
     CUtensorMap map_w_store;       // k_r4ring stores: the caller's state (kinetic destination, LB)
+    CUtensorMap map_t_load_pc;     // k_r4ring plane-contiguous layouts: LK view of the ping-pong buffer
+    CUtensorMap map_w_load_pc;     // and LP view of the caller's state
     const void* map_w_ptr;                 // state the W maps describe
     // CUDA graph of one Run() iteration, cached per (W, history, stream)
     cudaGraphExec_t graph;
@@ -1071,13 +1074,38 @@ static int encode_store_map(CUtensorMap* m, const void* base) {
     return WIG_OK;
 }
 
+// Plane-contiguous layouts of k_r4ring (LK = [y][x][p_y][p_x], LP =
+// [p_y][p_x][y][x]): a plane (f0, f1) of either half-step reads point (r, c)
+// at ((r * 64 + c) * 64 + f0) * 64 + f1, i.e. (2 float64 = 1 point, f1, f0, c,
+// r) with strides 16 B, 1 KB, 64 KB, 4 MB; the box is one plane.
+static int encode_plane_map_pc(CUtensorMap* m, const void* base) {
+    const cuuint64_t dims[5] = {2, 64, 64, 64, 64};
+    const cuuint64_t strides[4] = {16, 1024, 64 * 1024, 4 * 1024 * 1024};
+    const cuuint32_t box[5] = {2, 1, 1, 64, 64};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    EncodeTiledFn enc = encode_tiled_fn();
+    if (!enc) {
+        snprintf(wig_last_error_buffer(), 256, "cuTensorMapEncodeTiled is not available from the driver");
+        return WIG_ERR_CUDA;
+    }
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<void*>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(wig_last_error_buffer(), 256, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return WIG_ERR_CUDA;
+    }
+    return WIG_OK;
+}
+
 // LB maps of the caller's state W (the potential half-step's source, the
-// kinetic half-step's destination).
+// kinetic half-step's destination), and its LP map.
 static int ensure_w_maps(wig4d_plan* p, const void* W) {
     if (p->map_w_ptr == W) return WIG_OK;
     int s;
     if ((s = encode_plane_map(&p->map_w_load, W))) return s;
     if ((s = encode_store_map(&p->map_w_store, W))) return s;
+    if ((s = encode_plane_map_pc(&p->map_w_load_pc, W))) return s;
     p->map_w_ptr = W;
     return WIG_OK;
 }
@@ -1100,7 +1128,10 @@ static int ensure_r4ring(wig4d_plan* p) {
     int r;
     if ((r = ensure_r4t(p))) return r;
     if ((r = encode_store_map(&p->map_t_store, p->pingpong))) return r;
+    if ((r = encode_plane_map_pc(&p->map_t_load_pc, p->pingpong))) return r;
     const int sm = (int)r4ring::Cfg<double2>::SMEM;
+    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
@@ -1301,23 +1332,26 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             cudaFree(t64);
             if (!ok) { wig_set_cuda_error(cudaGetLastError(), "plane vectors"); free_plan(p); return WIG_ERR_CUDA; }
         }
-        // complex128: k_r4ring with TMA tensor stores (default); complex64:
-        // k_r4 with cluster stores.  WIG_FAST64_KERNEL overrides: r4 (k_r4,
-        // plain stores), r4cluster (k_r4, cluster stores), and for complex128
-        // r4t (TMA plane loads), r4ring (ring, per-thread stores), r4ring_ts
+        // complex128: k_r4ring on the plane-contiguous layouts (default);
+        // complex64: k_r4 with cluster stores.  WIG_FAST64_KERNEL overrides: r4
+        // (k_r4, plain stores), r4cluster (k_r4, cluster stores), and for
+        // complex128 r4t (TMA plane loads), r4ring (ring, per-thread stores),
+        // r4ring_ts (ring, TMA tensor stores on LA / LB), r4ring_pc
         const char* env_kern = getenv("WIG_FAST64_KERNEL");
-        const char* kern = env_kern ? env_kern : (desc->dtype == WIG_C128 ? "r4ring_ts" : "r4cluster");
+        const char* kern = env_kern ? env_kern : (desc->dtype == WIG_C128 ? "r4ring_pc" : "r4cluster");
         p->r4 = true;
         if (desc->dtype == WIG_C128 && strcmp(kern, "r4t") == 0) {
             int r;
             if ((r = ensure_r4t(p))) { free_plan(p); return r; }
             p->r4t = true;
         }
-        if (desc->dtype == WIG_C128 && (strcmp(kern, "r4ring") == 0 || strcmp(kern, "r4ring_ts") == 0)) {
+        if (desc->dtype == WIG_C128 && (strcmp(kern, "r4ring") == 0 || strcmp(kern, "r4ring_ts") == 0 ||
+                                        strcmp(kern, "r4ring_pc") == 0)) {
             int r;
             if ((r = ensure_r4ring(p))) { free_plan(p); return r; }
             p->r4ring = true;
-            p->r4ring_ts = strcmp(kern, "r4ring_ts") == 0;
+            p->r4ring_ts = strcmp(kern, "r4ring") != 0;
+            p->r4ring_pc = strcmp(kern, "r4ring_pc") == 0;
         }
         p->r4_cluster = strcmp(kern, "r4") != 0;
         if (cudaMalloc(&p->tw64, 64 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
@@ -1421,7 +1455,7 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     if (!p || !info) return WIG_ERR_INVALID_ARG;
     info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64;
-    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? 7 : (p->r4ring ? (p->r4ring_ts ? 9 : 8) : (p->r4t ? 4 : 3))));
+    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? 7 : (p->r4ring ? (p->r4ring_pc ? 10 : (p->r4ring_ts ? 9 : 8)) : (p->r4t ? 4 : 3))));
     return WIG_OK;
 }
 
@@ -1764,6 +1798,19 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
             const double2* pvp = pv + (size_t)p->shape[0] * p->shape[2] * 128;
             double2* P = reinterpret_cast<double2*>(p->pingpong);
             const double2 ks = make_double2(p->kin_scale, 0.0), ps = make_double2(p->pot_scale, 0.0);
+            if (p->r4ring_pc) {
+                // kinetic: LK (ping-pong) -> LP (W); potential: LP (W) -> LK (ping-pong)
+                if (part == 0)
+                    k_r4ring<double2, true, true, true><<<grid, K::NTH, K::SMEM, st>>>(
+                        p->map_t_load_pc, p->map_w_store, W, pv, tw, ks, p->cur_norm, p->ob, nullptr);
+                else if (part == 1)
+                    k_r4ring<double2, false, true, true><<<grid, K::NTH, K::SMEM, st>>>(
+                        p->map_w_load_pc, p->map_t_store, P, pvp, tw, ps, p->cur_norm, p->ob, p->partials);
+                else
+                    return fold_and_finalize(p, hist, rows, st);
+                WIG_LAUNCHED(part == 0 ? "k_r4ring<kin, pc>" : "k_r4ring<pot, pc>");
+                return WIG_OK;
+            }
             if (part == 0) {
                 if (p->r4ring_ts)
                     k_r4ring<double2, true, true><<<grid, K::NTH, K::SMEM, st>>>(p->map_t_load, p->map_w_store, W, pv,
@@ -1874,6 +1921,12 @@ static int enter_loop_layout(wig4d_plan* p, void* W, cudaStream_t st) {
         WIG_LAUNCHED("k_to_tc_layout");
         return WIG_OK;
     }
+    if (p->r4 && p->r4ring_pc) {
+        k_pc_transpose<double2, true><<<dim3(2, 2, 4096), 256, 0, st>>>((const double2*)W, (double2*)p->pingpong,
+                                                                         nullptr);
+        WIG_LAUNCHED("k_pc_transpose<to>");
+        return WIG_OK;
+    }
     if (p->r4) {
         if (p->dtype == WIG_C128)
             k_to_r4_layout<double2><<<wig_num_sms() * 8, 256, 0, st>>>((const double2*)W, (double2*)p->pingpong, p->npts);
@@ -1892,6 +1945,12 @@ static int leave_loop_layout(wig4d_plan* p, void* W, cudaStream_t st, bool divid
         k_from_tc_layout<<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)p->pingpong, (float2*)W, p->npts,
                                                             divide ? p->cur_norm : nullptr);
         WIG_LAUNCHED("k_from_tc_layout");
+        return WIG_OK;
+    }
+    if (p->r4 && p->r4ring_pc) {
+        k_pc_transpose<double2, false><<<dim3(2, 2, 4096), 256, 0, st>>>((const double2*)p->pingpong, (double2*)W,
+                                                                          divide ? p->cur_norm : nullptr);
+        WIG_LAUNCHED("k_pc_transpose<from>");
         return WIG_OK;
     }
     if (p->r4) {
@@ -1968,21 +2027,22 @@ struct TuneChoice { int engine, kin48, pot_gmax; };
 
 // engine: 0 k_r4 plain stores, 1 k_r4 cluster stores, 2 k_r4t, 3 k_tc64,
 // 4 the CUDA-core path of a plan without the 64^4 radix kernels, 5 k_r4ring,
-// 6 k_r4ring with TMA tensor stores
+// 6 k_r4ring with TMA tensor stores, 7 k_r4ring on the plane-contiguous layouts
 int apply_choice(wig4d_plan* p, const TuneChoice& c) {
     if (c.engine == 2) {
         const int r = ensure_r4t(p);
         if (r) return r;
     }
-    if (c.engine == 5 || c.engine == 6) {
+    if (c.engine >= 5 && c.engine <= 7) {
         const int r = ensure_r4ring(p);
         if (r) return r;
     }
     p->tc = c.engine == 3;
     p->r4_cluster = c.engine == 1;
     p->r4t = c.engine == 2;
-    p->r4ring = c.engine == 5 || c.engine == 6;
-    p->r4ring_ts = c.engine == 6;
+    p->r4ring = c.engine >= 5 && c.engine <= 7;
+    p->r4ring_ts = c.engine == 6 || c.engine == 7;
+    p->r4ring_pc = c.engine == 7;
     p->kin48 = c.kin48 != 0;
     p->pot_gmax = c.pot_gmax;
     if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
@@ -1991,7 +2051,7 @@ int apply_choice(wig4d_plan* p, const TuneChoice& c) {
 
 TuneChoice current_choice(const wig4d_plan* p) {
     TuneChoice c;
-    c.engine = p->tc ? 3 : (p->r4 ? (p->r4ring ? (p->r4ring_ts ? 6 : 5) : (p->r4t ? 2 : (p->r4_cluster ? 1 : 0))) : 4);
+    c.engine = p->tc ? 3 : (p->r4 ? (p->r4ring ? (p->r4ring_pc ? 7 : (p->r4ring_ts ? 6 : 5)) : (p->r4t ? 2 : (p->r4_cluster ? 1 : 0))) : 4);
     c.kin48 = p->kin48;
     c.pot_gmax = p->pot_gmax;
     return c;
@@ -2031,6 +2091,7 @@ extern "C" int wig4d_autotune(wig4d_plan* p, int iterations, int flags, void* st
         if (p->dtype == WIG_C128) engines.push_back({2, base.kin48, base.pot_gmax});
         if (p->dtype == WIG_C128) engines.push_back({5, base.kin48, base.pot_gmax});
         if (p->dtype == WIG_C128) engines.push_back({6, base.kin48, base.pot_gmax});
+        if (p->dtype == WIG_C128) engines.push_back({7, base.kin48, base.pot_gmax});
     } else {
         engines.push_back({4, base.kin48, base.pot_gmax});
     }

@@ -51,7 +51,7 @@ def test_c128_and_tc_vs_oracle_20_iterations_64():
     W0 = cat_xp(f128._coords, c)
     Wo, obs = o.run(W0, 19)
     f128 = _run(p, W0, 20)
-    assert f128.plan_info()["run64_kernel"] == "r4ring_ts"
+    assert f128.plan_info()["run64_kernel"] == "r4ring_pc"
     for name in OBS:
         assert rel_err(getattr(f128, name), obs[name]) < 1e-12, name
     assert rel_err(f128.norm, obs["norms"]) < 1e-12

@@ -302,12 +302,13 @@ def test_k48_matches_generic(dtype, tol, monkeypatch):
         assert rel_err(a, b) < tol
 
 
-@pytest.mark.parametrize("variant", ["r4t", "r4", "r4cluster", "r4ring"])
+@pytest.mark.parametrize("variant", ["r4t", "r4", "r4cluster", "r4ring", "r4ring_ts"])
 def test_r4_variants_match_default(variant, monkeypatch):
     """complex128: k_r4 with TMA plane loads (r4t), k_r4 with plain (r4) or
-    cluster (r4cluster) stores and k_r4ring with per-thread stores against
-    the default, k_r4ring with TMA tensor stores: the same arithmetic (the
-    ring kernels sum each plane's observables in another order)."""
+    cluster (r4cluster) stores, k_r4ring with per-thread stores (r4ring) or
+    TMA tensor stores (r4ring_ts) on LA / LB, against the default, k_r4ring
+    on the plane-contiguous layouts: the same arithmetic (the ring kernels
+    sum each plane's observables in another order)."""
     from configs import cat_xp
     p, c = config2(7, 64)
     f1 = make_frame(GPU_Wigner4D, p)
@@ -315,7 +316,7 @@ def test_r4_variants_match_default(variant, monkeypatch):
     f2 = make_frame(GPU_Wigner4D, p)
     monkeypatch.delenv("WIG_FAST64_KERNEL")
     label = {"r4cluster": "r4"}.get(variant, variant)
-    assert (f1.plan_info()["run64_kernel"], f2.plan_info()["run64_kernel"]) == ("r4ring_ts", label)
+    assert (f1.plan_info()["run64_kernel"], f2.plan_info()["run64_kernel"]) == ("r4ring_pc", label)
     W0 = cat_xp(f1._coords, c)
     for f in (f1, f2):
         f.W_init_gpu.set(W0)
