@@ -563,7 +563,9 @@ def main():
     hmx = histmx[:K].cpu().numpy()
     kmx, pmx, _ = [m / K for m in fmx.run_device_timed(fmx.W_init_gpu, K, histmx)]
     dmx = max(kmx, pmx)
-    mixed_form = {"dtype": "c64 state, FP64 transforms and factors", "kernel": "k_r4<double2, ., ., float2>",
+    mx_kernel = {"r4ring_mx": "k_r4ring_mx", "r4_mixed": "k_r4<double2, ., ., float2>"}.get(
+        fmx.plan_info()["run64_kernel"], fmx.plan_info()["run64_kernel"])
+    mixed_form = {"dtype": "c64 state, FP64 transforms and factors", "kernel": mx_kernel,
                   "steps_per_s": K / (msmx / 1e3), "speedup_vs_plain": (K / (msmx / 1e3)) / (K / (ms / 1e3)),
                   "kinetic_ms": kmx, "potential_ms": pmx,
                   "roofline": {"bound": "hbm", "achieved": state_bytes / (dmx / 1e3) / 1e9, "peak": peak,

@@ -889,6 +889,199 @@ __global__ void __launch_bounds__(256) k_pc_transpose(const C* __restrict__ src,
     }
 }
 
+// ---------------------------------------------------------------------------
+// k_r4ring_mx: the mixed form (complex64 state in memory, complex128
+// arithmetic) on the plane-contiguous layouts LK / LP.
+//
+// A complex64 point is 8 bytes, less than the 16 bytes a tensor box row
+// needs, so the unit's two planes (f1 = 2m, 2m + 1: neighbours in memory) come
+// in one box of two-point rows, 64 KB laid out [r][c][plane].  One CTA per SM,
+// two groups of 256 threads, group g on plane g of every unit; each group has
+// its own 64 KB complex128 exchange plane.  Both groups read their plane out
+// of the landing box, then (one CTA barrier) thread 0 refills the box with
+// the CTA's next unit, which lands while both planes are transformed.  Each
+// result is staged as complex64 [r][c] in the group's exchange plane and
+// written by one 32 KB bulk copy (the plane is contiguous); the group's next
+// first exchange waits until that copy has read the plane.
+// The box's wait is bounded and decided by the whole CTA (__syncthreads_and):
+// on a timeout the CTA poisons the norm or the partial row with NaN and
+// stops; before it exits, thread 0 waits (bounded) for a copy still in flight.
+// ---------------------------------------------------------------------------
+namespace r4mx {
+constexpr int NTH = 2 * r4::NT;
+constexpr size_t BOX = 2 * 4096 * sizeof(float2);                     // 64 KB
+constexpr size_t EX_OFF = BOX;                                         // 2 x 64 KB complex128
+constexpr size_t TW_OFF = EX_OFF + 2 * 4096 * sizeof(double2);
+constexpr size_t PV_OFF = TW_OFF + 64 * sizeof(double2);
+constexpr size_t RED_OFF = PV_OFF + 2 * 128 * sizeof(double2);
+constexpr size_t BAR_OFF = RED_OFF + 2 * 8 * 16 * sizeof(double);
+constexpr size_t SMEM = BAR_OFF + 64 + 128;
+static_assert(SMEM <= 232448, "k_r4ring_mx shared memory");
+}  // namespace r4mx
+
+template <bool KIN>
+__global__ void __launch_bounds__(r4mx::NTH, 1)
+k_r4ring_mx(const __grid_constant__ CUtensorMap src_map, float2* __restrict__ dst, const double2* __restrict__ PV,
+            const double2* __restrict__ gtw, double2 scale, double* __restrict__ d_norm, ObsTabs ob,
+            double* __restrict__ partials) {
+    using namespace r4;
+    using namespace r4t;
+    using namespace r4ring;
+    typedef double2 C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+    const float2* box = reinterpret_cast<const float2*>(base);
+    C* tw = reinterpret_cast<C*>(base + r4mx::TW_OFF);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(base + r4mx::BAR_OFF);
+    const int tid = threadIdx.x, g = tid >> 8, t = tid & (NT - 1), lane = t & 31, wp = t >> 5;
+    C* s = reinterpret_cast<C*>(base + r4mx::EX_OFF) + g * 4096;
+    double2* pvs = reinterpret_cast<double2*>(base + r4mx::PV_OFF) + g * 128;
+    double* red = reinterpret_cast<double*>(base + r4mx::RED_OFF) + g * 128;
+    const int nunits = 2048;
+    const int nloc = (int)blockIdx.x < nunits ? (nunits - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    auto unit_of = [&](int n) { return (int)blockIdx.x + n * (int)gridDim.x; };
+    auto load_unit = [&](int n) {
+        const int u = unit_of(n), f0 = u >> 5, m = u & 31;      // planes (f0, 2m) and (f0, 2m + 1)
+        fence_async_smem();
+        mbar_expect_tx(bar, (uint32_t)r4mx::BOX);
+        tma_load_5d(base, &src_map, 0, m, f0, 0, 0, bar);
+    };
+    if (tid == 0) {
+        mbar_init(bar);
+        fence_async_smem();
+        if (nloc > 0) load_unit(0);
+    }
+    if (tid < 64) load_tw(tw, gtw, tid);
+    double2 cc = scale;
+    if (KIN) cc = zmul(cc, zinv(make_double2(d_norm[0], d_norm[1])));
+    const int ac = t & 15, ar = t >> 4;
+    const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
+    bool stored = false;                               // thread 0 of a group: a bulk copy may be reading s
+    int aborted_at = -1;                               // the unit whose box did not arrive
+    __syncthreads();                                   // barrier initialised, twiddles ready
+    for (int n = 0; n < nloc; ++n) {
+        const int pl = 2 * unit_of(n) + g;             // plane (f0, f1) = (pl >> 6, pl & 63)
+        if (t < 128) pvs[t < 64 ? t : 64 + (t & 48) + ((t & 3) << 2) + ((t >> 2) & 3)] = __ldg(PV + (long long)pl * 128 + t);
+        bool arrived = false;
+        for (int it = 0; it < (1 << 22) && !arrived; ++it) arrived = mbar_try_wait(bar, (uint32_t)(n & 1));
+        if (!__syncthreads_and(arrived ? 1 : 0)) {
+            if (t == 0) {
+                if (KIN) d_norm[0] = __longlong_as_double(0x7ff8000000000000LL);
+                else partials[(long long)pl * NPART] = __longlong_as_double(0x7ff8000000000000LL);
+            }
+            aborted_at = n;
+            break;
+        }
+        C v[16];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[4 * i + j] = widen<C>(box[((ar + 16 * i) * 64 + ac + 16 * j) * 2 + g]);
+        __syncthreads();                               // both planes have been read out of the box
+        if (tid == 0 && n + 1 < nloc) load_unit(n + 1);
+        // ---- forward
+        pass<C, true>(v);
+        twiddle<C, true>(v, tw, ac, ar);
+        if (t == 0 && stored) {
+            bulk_wait_read();                          // the previous plane's copy has left s
+            stored = false;
+        }
+        group_sync(g);
+        put(s, L1, v);
+        group_sync(g);
+        get(s, L2, v);
+        pass<C, true>(v);
+        twiddle<C, true>(v, tw, 4 * (t & 3), 4 * ((t >> 4) & 3));
+        group_sync(g);
+        put(s, L2, v);
+        group_sync(g);
+        get(s, L3, v);
+        pass<C, true>(v);
+        {
+            const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
+            double2 b[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = pvs[64 + 16 * j + 4 * c2 + c1];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const double2 a = zmul(pvs[r2 + 4 * r1 + 16 * i], cc);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) factor_mul(v[4 * i + j], a, b[j]);
+            }
+        }
+        // ---- inverse
+        pass<C, false>(v);
+        twiddle<C, false>(v, tw, ((t >> 2) & 3) + 4 * (t & 3), (t >> 6) + 4 * ((t >> 4) & 3));
+        group_sync(g);
+        put(s, L3, v);
+        group_sync(g);
+        get(s, L2, v);
+        pass<C, false>(v);
+        twiddle<C, false>(v, tw, 4 * ((t >> 2) & 3), 4 * (t >> 6));
+        group_sync(g);
+        put(s, L2, v);
+        group_sync(g);
+        get(s, L1, v);
+        pass<C, false>(v);
+        group_sync(g);                                 // the last exchange has been read
+        {
+            float2* sf = reinterpret_cast<float2*>(s);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) sf[(ar + 16 * i) * 64 + ac + 16 * j] = narrow<float2>(v[4 * i + j]);
+            fence_async_smem();
+            group_sync(g);
+            if (t == 0) {
+                bulk_store_1d(dst + (long long)pl * 4096, sf, (uint32_t)(4096 * sizeof(float2)));
+                stored = true;
+            }
+        }
+        if (!KIN) {
+            // observables of the new (x, p) state: p_y = ar + 16 i, p_x = ac + 16 j
+            // (the complex128 values before rounding, as k_r4<double2, ., ., float2>)
+            double a[NPART];
+#pragma unroll
+            for (int q = 0; q < NPART; ++q) a[q] = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const double qy = __ldg(ob.cpy + ar + 16 * i);
+                double w0x = 0, w0y = 0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const C w = v[4 * i + j];
+                    const double qx = __ldg(ob.cpx + ac + 16 * j), kk = __ldg(ob.ep + (ar + 16 * i) * 64 + ac + 16 * j);
+                    w0x += w.x; w0y += w.y;
+                    a[2] += qx * w.x; a[3] += qx * w.y;
+                    a[4] += qx * qx * w.x; a[5] += qx * qx * w.y;
+                    a[10] += kk * w.x; a[11] += kk * w.y;
+                }
+                a[0] += w0x; a[1] += w0y;
+                a[6] += qy * w0x; a[7] += qy * w0y;
+                a[8] += qy * qy * w0x; a[9] += qy * qy * w0y;
+            }
+            double d[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) d[q] = q < NPART ? a[q] : 0.0;
+            const double sum = warp_slot_sums(d, lane);
+            if (!(lane & 1)) red[wp * 16 + (lane >> 1)] = sum;
+            group_sync(g);
+            if (t < NPART) {
+                double tot = 0.0;
+#pragma unroll
+                for (int w = 0; w < NT / 32; ++w) tot += red[w * 16 + t];
+                partials[(long long)pl * NPART + t] = tot;
+            }
+        }
+    }
+    if (t == 0) bulk_wait_all();                       // every copy of this group has completed
+    if (tid == 0 && aborted_at >= 0) {
+        // the timed-out unit's copy (the last one issued) may still be in flight
+        for (int it = 0; it < (1 << 22); ++it)
+            if (mbar_try_wait(bar, (uint32_t)(aborted_at & 1))) break;
+    }
+}
+
 // The 64-entry twiddle table of k_r4 / k_r4t, built once per plan.
 template <class C>
 __global__ void k_make_r4_twiddles(C* tw) { r4::make_tw<C>(tw); }

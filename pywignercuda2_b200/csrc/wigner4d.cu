@@ -754,6 +754,10 @@ struct wig4d_plan {
     bool r4ring_ts;                // k_r4ring with TMA tensor stores
     bool r4ring_pc;                // k_r4ring on the plane-contiguous layouts LK / LP (bulk stores)
     bool r4_mixed;                 // complex64 64^4: k_r4 with FP64 transforms on complex64 storage
+    bool mx_ring;                  // the mixed form with k_r4ring_mx on the plane-contiguous layouts
+    CUtensorMap map_t_load_mx;     // k_r4ring_mx: unit boxes of the ping-pong buffer (LK)
+    CUtensorMap map_w_load_mx;     // and of the caller's state (LP)
+    const void* map_w_mx_ptr;      // state map_w_load_mx describes
     void* tw64d;                   // its FP64 twiddle table
     int dense_n;                   // > 0: general-delta half-steps fused (k_dense_half, N^4 grids)
     const void* dmat[4];           // FAFT matrices per axis (|delta|), when dense_n > 0
@@ -1089,6 +1093,29 @@ static int encode_plane_map_pc(CUtensorMap* m, const void* base) {
         return WIG_ERR_CUDA;
     }
     const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<void*>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(wig_last_error_buffer(), 256, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return WIG_ERR_CUDA;
+    }
+    return WIG_OK;
+}
+
+// The mixed form's unit boxes on LK / LP (complex64): the two planes f1 = 2m,
+// 2m + 1 of one f0 as rows of two points, (4 float32, f1 / 2, f0, c, r) with
+// strides 16 B, 512 B, 32 KB, 2 MB; the box is one unit (64 KB).
+static int encode_unit_map_mx(CUtensorMap* m, const void* base) {
+    const cuuint64_t dims[5] = {4, 32, 64, 64, 64};
+    const cuuint64_t strides[4] = {16, 512, 32 * 1024, 2 * 1024 * 1024};
+    const cuuint32_t box[5] = {4, 1, 1, 64, 64};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    EncodeTiledFn enc = encode_tiled_fn();
+    if (!enc) {
+        snprintf(wig_last_error_buffer(), 256, "cuTensorMapEncodeTiled is not available from the driver");
+        return WIG_ERR_CUDA;
+    }
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, const_cast<void*>(base), dims, strides, box, estr,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
@@ -1438,6 +1465,15 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
         cudaFuncSetAttribute(k_r4<double2, true, true, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
         cudaFuncSetAttribute(k_r4<double2, false, true, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, rsm);
         p->r4_mixed = true;
+        // k_r4ring_mx by default; WIG_MIXED_KERNEL=r4 keeps k_r4<double2, ., ., float2>
+        const char* mk = getenv("WIG_MIXED_KERNEL");
+        if (!(mk && strcmp(mk, "r4") == 0)) {
+            int r;
+            if ((r = encode_unit_map_mx(&p->map_t_load_mx, p->pingpong))) { free_plan(p); return r; }
+            cudaFuncSetAttribute(k_r4ring_mx<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4mx::SMEM);
+            cudaFuncSetAttribute(k_r4ring_mx<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4mx::SMEM);
+            p->mx_ring = true;
+        }
     }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) { wig_set_cuda_error(e, "wig4d_plan_create"); free_plan(p); return WIG_ERR_CUDA; }
@@ -1455,7 +1491,7 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     if (!p || !info) return WIG_ERR_INVALID_ARG;
     info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64;
-    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? 7 : (p->r4ring ? (p->r4ring_pc ? 10 : (p->r4ring_ts ? 9 : 8)) : (p->r4t ? 4 : 3))));
+    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? (p->mx_ring ? 11 : 7) : (p->r4ring ? (p->r4ring_pc ? 10 : (p->r4ring_ts ? 9 : 8)) : (p->r4t ? 4 : 3))));
     return WIG_OK;
 }
 
@@ -1856,6 +1892,33 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
         }
     }
     if constexpr (std::is_same<C, float2>::value) {
+        if (p->r4 && p->mx_ring) {
+            // complex64 LK / LP layouts, FP64 transforms: kinetic LK (ping-pong) -> LP (W),
+            // potential LP (W) -> LK (ping-pong)
+            if (p->map_w_mx_ptr != (const void*)W) {
+                int s;
+                if ((s = encode_unit_map_mx(&p->map_w_load_mx, W))) return s;
+                p->map_w_mx_ptr = W;
+            }
+            float2* P = reinterpret_cast<float2*>(p->pingpong);
+            const double2* pv = reinterpret_cast<const double2*>(p->pv);
+            const double2* tw = reinterpret_cast<const double2*>(p->tw64d);
+            const unsigned grid = (unsigned)(wig_num_sms() < 2048 ? wig_num_sms() : 2048);
+            if (part == 0) {
+                k_r4ring_mx<true><<<grid, r4mx::NTH, r4mx::SMEM, st>>>(p->map_t_load_mx, W, pv, tw,
+                                                                       make_double2(p->kin_scale, 0.0), p->cur_norm,
+                                                                       p->ob, nullptr);
+                WIG_LAUNCHED("k_r4ring_mx<kin>");
+            } else if (part == 1) {
+                k_r4ring_mx<false><<<grid, r4mx::NTH, r4mx::SMEM, st>>>(
+                    p->map_w_load_mx, P, pv + (size_t)p->shape[0] * p->shape[2] * 128, tw,
+                    make_double2(p->pot_scale, 0.0), p->cur_norm, p->ob, p->partials);
+                WIG_LAUNCHED("k_r4ring_mx<pot>");
+            } else {
+                return fold_and_finalize(p, hist, rows, st);
+            }
+            return WIG_OK;
+        }
         if (p->r4 && p->r4_mixed) {
             // complex64 LA / LB layouts, FP64 transforms
             float2* P = reinterpret_cast<float2*>(p->pingpong);
@@ -1921,6 +1984,12 @@ static int enter_loop_layout(wig4d_plan* p, void* W, cudaStream_t st) {
         WIG_LAUNCHED("k_to_tc_layout");
         return WIG_OK;
     }
+    if (p->r4 && p->mx_ring) {
+        k_pc_transpose<float2, true><<<dim3(2, 2, 4096), 256, 0, st>>>((const float2*)W, (float2*)p->pingpong,
+                                                                        nullptr);
+        WIG_LAUNCHED("k_pc_transpose<to>");
+        return WIG_OK;
+    }
     if (p->r4 && p->r4ring_pc) {
         k_pc_transpose<double2, true><<<dim3(2, 2, 4096), 256, 0, st>>>((const double2*)W, (double2*)p->pingpong,
                                                                          nullptr);
@@ -1945,6 +2014,12 @@ static int leave_loop_layout(wig4d_plan* p, void* W, cudaStream_t st, bool divid
         k_from_tc_layout<<<wig_num_sms() * 8, 256, 0, st>>>((const float2*)p->pingpong, (float2*)W, p->npts,
                                                             divide ? p->cur_norm : nullptr);
         WIG_LAUNCHED("k_from_tc_layout");
+        return WIG_OK;
+    }
+    if (p->r4 && p->mx_ring) {
+        k_pc_transpose<float2, false><<<dim3(2, 2, 4096), 256, 0, st>>>((const float2*)p->pingpong, (float2*)W,
+                                                                         divide ? p->cur_norm : nullptr);
+        WIG_LAUNCHED("k_pc_transpose<from>");
         return WIG_OK;
     }
     if (p->r4 && p->r4ring_pc) {

@@ -107,14 +107,18 @@ def test_tc_rejects_unsupported_plans(dtype, n):
     assert e.value.status == 2
 
 
-def test_mixed_form_vs_oracle_20_iterations_64():
-    """complex64 storage with FP64 transforms (fp64_transforms = True): the
-    only rounding left is the state's float32 storage, relative to each
-    value, so the energy stays within 1e-6 of the oracle."""
+@pytest.mark.parametrize("kernel", ["r4ring_mx", "r4_mixed"])
+def test_mixed_form_vs_oracle_20_iterations_64(kernel, monkeypatch):
+    """complex64 storage with FP64 transforms (fp64_transforms = True), on
+    the plane-contiguous ring kernel (default) or on k_r4 (WIG_MIXED_KERNEL
+    = r4): the only rounding left is the state's float32 storage, relative
+    to each value, so the energy stays within 1e-6 of the oracle."""
+    if kernel == "r4_mixed":
+        monkeypatch.setenv("WIG_MIXED_KERNEL", "r4")
     p, c = config2(0, 64)
     o = Wigner4DOracle(p)
     f = make_frame(GPU_Wigner4D, p, complex_dtype=np.complex64, fp64_transforms=True)
-    assert f.plan_info()["run64_kernel"] == "r4_mixed"
+    assert f.plan_info()["run64_kernel"] == kernel
     W0 = cat_xp(f._coords, c)
     Wo, obs = o.run(W0.astype(np.complex64).astype(np.complex128), 19)
     f = _run(p, W0, 20, complex_dtype=np.complex64, fp64_transforms=True)
