@@ -405,7 +405,7 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--no-dirac", action="store_true", help="skip the Wigner-Dirac line")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the 1000-step accuracy block")
-    ap.add_argument("--profile-form", choices=["c128", "c64", "tc", "tc-general"],
+    ap.add_argument("--profile-form", choices=["c128", "c64", "tc", "tc-general", "mixed"],
                     help="only run two Run() iterations of one 64^4 form (a small case for ncu) and exit")
     ap.add_argument("--dirac-steps", type=int, default=20)
     ap.add_argument("--dirac-passes", choices=["c128", "c64"],
@@ -417,7 +417,8 @@ def main():
     if args.profile_form:
         kw = {"c128": {}, "c64": {"complex_dtype": np.complex64},
               "tc": {"complex_dtype": np.complex64, "tensor_cores": True},
-              "tc-general": {"complex_dtype": np.complex64, "tensor_cores": True}}[args.profile_form]
+              "tc-general": {"complex_dtype": np.complex64, "tensor_cores": True},
+              "mixed": {"complex_dtype": np.complex64, "fp64_transforms": True}}[args.profile_form]
         from configs import config2
         from frames import make_frame
         from pywignercuda2_b200 import GPU_Wigner4D
