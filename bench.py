@@ -571,7 +571,9 @@ def main():
                   "kinetic_ms": kmx, "potential_ms": pmx,
                   "roofline": {"bound": "hbm", "achieved": state_bytes / (dmx / 1e3) / 1e9, "peak": peak,
                                "unit": "GB/s", "frac": state_bytes / (dmx / 1e3) / 1e9 / peak,
-                               "algorithmic_bytes_per_launch": state_bytes},
+                               "algorithmic_bytes_per_launch": state_bytes,
+                               "traffic": _traffic().get((mx_kernel + ("<pot>" if pmx >= kmx else "<kin>"),
+                                                          "64x64x64x64_c64"))},
                   "error_vs_c128": dict(_hist_err(hmx, h128), steps=Wm + K)}
     del fmx
 
