@@ -540,7 +540,7 @@ def main():
                 "step_frac": (4 * state_bytes / (ms / K / 1e3) / 1e9) / peak}
     k32, p32, _ = [m / K for m in f32.run_device_timed(f32.W_init_gpu, K, hist32)]
     d32 = max(k32, p32)
-    kname = "k_r4"
+    kname = "k_r4ring_mx" if f32.plan_info()["run64_kernel"] == "r4ring_f32" else "k_r4"
     precision["roofline"] = {"bound": "hbm", "kernel": kname + ("<pot>" if p32 >= k32 else "<kin>"),
                              "achieved": state_bytes / (d32 / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                              "frac": state_bytes / (d32 / 1e3) / 1e9 / peak,

@@ -271,7 +271,8 @@ int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
    with TMA tensor stores (WIG_FAST64_KERNEL=r4ring_ts), 10 k_r4ring on the
    plane-contiguous layouts with bulk stores (the complex128 default), 11
    k_r4ring_mx (the mixed form of wig4d_desc.transform = 3 on the
-   plane-contiguous layouts; WIG_MIXED_KERNEL=r4 selects 7). */
+   plane-contiguous layouts; WIG_MIXED_KERNEL=r4 selects 7), 12 the same
+   ring with float32 arithmetic for complex64 (WIG_FAST64_KERNEL=r4ring_f32). */
 int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
 
 

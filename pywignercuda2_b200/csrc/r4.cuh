@@ -919,22 +919,24 @@ constexpr size_t SMEM = BAR_OFF + 64 + 128;
 static_assert(SMEM <= 232448, "k_r4ring_mx shared memory");
 }  // namespace r4mx
 
-template <bool KIN>
+// C: the arithmetic type, double2 (the mixed form) or float2 (the complex64
+// radix form on the same layouts; exchanges in the first 32 KB of each
+// group's plane, twiddles from the normalised float32 table).
+template <class C, bool KIN>
 __global__ void __launch_bounds__(r4mx::NTH, 1)
 k_r4ring_mx(const __grid_constant__ CUtensorMap src_map, float2* __restrict__ dst, const double2* __restrict__ PV,
-            const double2* __restrict__ gtw, double2 scale, double* __restrict__ d_norm, ObsTabs ob,
+            const C* __restrict__ gtw, double2 scale, double* __restrict__ d_norm, ObsTabs ob,
             double* __restrict__ partials) {
     using namespace r4;
     using namespace r4t;
     using namespace r4ring;
-    typedef double2 C;
     extern __shared__ __align__(16) unsigned char smraw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
     const float2* box = reinterpret_cast<const float2*>(base);
     C* tw = reinterpret_cast<C*>(base + r4mx::TW_OFF);
     uint64_t* bar = reinterpret_cast<uint64_t*>(base + r4mx::BAR_OFF);
     const int tid = threadIdx.x, g = tid >> 8, t = tid & (NT - 1), lane = t & 31, wp = t >> 5;
-    C* s = reinterpret_cast<C*>(base + r4mx::EX_OFF) + g * 4096;
+    C* s = reinterpret_cast<C*>(base + r4mx::EX_OFF + (size_t)g * 4096 * sizeof(double2));
     double2* pvs = reinterpret_cast<double2*>(base + r4mx::PV_OFF) + g * 128;
     double* red = reinterpret_cast<double*>(base + r4mx::RED_OFF) + g * 128;
     const int nunits = 2048;
@@ -1039,7 +1041,7 @@ k_r4ring_mx(const __grid_constant__ CUtensorMap src_map, float2* __restrict__ ds
         }
         if (!KIN) {
             // observables of the new (x, p) state: p_y = ar + 16 i, p_x = ac + 16 j
-            // (the complex128 values before rounding, as k_r4<double2, ., ., float2>)
+            // (the values before rounding to the storage type, as k_r4 sums them)
             double a[NPART];
 #pragma unroll
             for (int q = 0; q < NPART; ++q) a[q] = 0;

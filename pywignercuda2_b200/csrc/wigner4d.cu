@@ -755,6 +755,7 @@ struct wig4d_plan {
     bool r4ring_pc;                // k_r4ring on the plane-contiguous layouts LK / LP (bulk stores)
     bool r4_mixed;                 // complex64 64^4: k_r4 with FP64 transforms on complex64 storage
     bool mx_ring;                  // the mixed form with k_r4ring_mx on the plane-contiguous layouts
+    bool mx_f32;                   // ... with float32 arithmetic: the complex64 radix form on those layouts
     CUtensorMap map_t_load_mx;     // k_r4ring_mx: unit boxes of the ping-pong buffer (LK)
     CUtensorMap map_w_load_mx;     // and of the caller's state (LP)
     const void* map_w_mx_ptr;      // state map_w_load_mx describes
@@ -1381,6 +1382,14 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
             p->r4ring_pc = strcmp(kern, "r4ring_pc") == 0;
         }
         p->r4_cluster = strcmp(kern, "r4") != 0;
+        if (desc->dtype == WIG_C64 && strcmp(kern, "r4ring_f32") == 0) {
+            int r;
+            if ((r = encode_unit_map_mx(&p->map_t_load_mx, p->pingpong))) { free_plan(p); return r; }
+            cudaFuncSetAttribute(k_r4ring_mx<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4mx::SMEM);
+            cudaFuncSetAttribute(k_r4ring_mx<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4mx::SMEM);
+            p->mx_ring = true;
+            p->mx_f32 = true;
+        }
         if (cudaMalloc(&p->tw64, 64 * esz) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
         if (cudaMalloc(&p->fold, FOLD_BLOCKS * NSUM * sizeof(double)) != cudaSuccess) { free_plan(p); return WIG_ERR_ALLOC; }
         if (desc->dtype == WIG_C128) k_make_r4_twiddles<double2><<<1, 64>>>((double2*)p->tw64);
@@ -1470,8 +1479,8 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
         if (!(mk && strcmp(mk, "r4") == 0)) {
             int r;
             if ((r = encode_unit_map_mx(&p->map_t_load_mx, p->pingpong))) { free_plan(p); return r; }
-            cudaFuncSetAttribute(k_r4ring_mx<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4mx::SMEM);
-            cudaFuncSetAttribute(k_r4ring_mx<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4mx::SMEM);
+            cudaFuncSetAttribute(k_r4ring_mx<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4mx::SMEM);
+            cudaFuncSetAttribute(k_r4ring_mx<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4mx::SMEM);
             p->mx_ring = true;
         }
     }
@@ -1491,7 +1500,7 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     if (!p || !info) return WIG_ERR_INVALID_ARG;
     info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64;
-    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? (p->mx_ring ? 11 : 7) : (p->r4ring ? (p->r4ring_pc ? 10 : (p->r4ring_ts ? 9 : 8)) : (p->r4t ? 4 : 3))));
+    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? (p->mx_ring ? 11 : 7) : p->mx_f32 ? 12 : (p->r4ring ? (p->r4ring_pc ? 10 : (p->r4ring_ts ? 9 : 8)) : (p->r4t ? 4 : 3))));
     return WIG_OK;
 }
 
@@ -1902,17 +1911,26 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
             }
             float2* P = reinterpret_cast<float2*>(p->pingpong);
             const double2* pv = reinterpret_cast<const double2*>(p->pv);
+            const double2* pvp = pv + (size_t)p->shape[0] * p->shape[2] * 128;
             const double2* tw = reinterpret_cast<const double2*>(p->tw64d);
+            const float2* tw32 = reinterpret_cast<const float2*>(p->tw64);
+            const double2 ks = make_double2(p->kin_scale, 0.0), ps = make_double2(p->pot_scale, 0.0);
             const unsigned grid = (unsigned)(wig_num_sms() < 2048 ? wig_num_sms() : 2048);
             if (part == 0) {
-                k_r4ring_mx<true><<<grid, r4mx::NTH, r4mx::SMEM, st>>>(p->map_t_load_mx, W, pv, tw,
-                                                                       make_double2(p->kin_scale, 0.0), p->cur_norm,
-                                                                       p->ob, nullptr);
+                if (p->mx_f32)
+                    k_r4ring_mx<float2, true><<<grid, r4mx::NTH, r4mx::SMEM, st>>>(p->map_t_load_mx, W, pv, tw32, ks,
+                                                                                   p->cur_norm, p->ob, nullptr);
+                else
+                    k_r4ring_mx<double2, true><<<grid, r4mx::NTH, r4mx::SMEM, st>>>(p->map_t_load_mx, W, pv, tw, ks,
+                                                                                    p->cur_norm, p->ob, nullptr);
                 WIG_LAUNCHED("k_r4ring_mx<kin>");
             } else if (part == 1) {
-                k_r4ring_mx<false><<<grid, r4mx::NTH, r4mx::SMEM, st>>>(
-                    p->map_w_load_mx, P, pv + (size_t)p->shape[0] * p->shape[2] * 128, tw,
-                    make_double2(p->pot_scale, 0.0), p->cur_norm, p->ob, p->partials);
+                if (p->mx_f32)
+                    k_r4ring_mx<float2, false><<<grid, r4mx::NTH, r4mx::SMEM, st>>>(p->map_w_load_mx, P, pvp, tw32, ps,
+                                                                                    p->cur_norm, p->ob, p->partials);
+                else
+                    k_r4ring_mx<double2, false><<<grid, r4mx::NTH, r4mx::SMEM, st>>>(p->map_w_load_mx, P, pvp, tw, ps,
+                                                                                     p->cur_norm, p->ob, p->partials);
                 WIG_LAUNCHED("k_r4ring_mx<pot>");
             } else {
                 return fold_and_finalize(p, hist, rows, st);

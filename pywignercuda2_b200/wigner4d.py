@@ -347,7 +347,7 @@ class GPU_Wigner4D:
         info = (ctypes.c_int * 4)()
         _lib.call("wig4d_plan_info", self._plan, info)
         run64 = {0: None, 3: "r4", 4: "r4t", 6: "tc", 7: "r4_mixed", 8: "r4ring", 9: "r4ring_ts", 10: "r4ring_pc",
-                 11: "r4ring_mx"}[info[3]]
+                 11: "r4ring_mx", 12: "r4ring_f32"}[info[3]]
         return {"fused_kinetic": bool(info[0]), "fused_potential": bool(info[1]), "fast64": bool(info[2]),
                 "run64_kernel": run64}
 

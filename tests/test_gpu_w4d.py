@@ -247,12 +247,18 @@ def test_run_timed_matches_run(n, dtype):
     assert all(m > 0 for m in ms)
 
 
-def test_run_r4_c64_vs_oracle():
-    """complex64 at 64^4 runs k_r4 on the LA / LB layouts; the state comes
-    back in the reference layout.  Float32 bar: 2e-5 relative after 3 steps."""
+@pytest.mark.parametrize("kernel", ["r4", "r4ring_f32"])
+def test_run_r4_c64_vs_oracle(kernel, monkeypatch):
+    """complex64 at 64^4 runs k_r4 on the LA / LB layouts (default) or the
+    float32 ring on the plane-contiguous layouts (WIG_FAST64_KERNEL =
+    r4ring_f32); the state comes back in the reference layout.  Float32 bar:
+    2e-5 relative after 3 steps."""
     from configs import cat_xp
+    if kernel == "r4ring_f32":
+        monkeypatch.setenv("WIG_FAST64_KERNEL", kernel)
     p, c = config2(2, 64)
     f, o = _pair(p, np.complex64)
+    assert f.plan_info()["run64_kernel"] == kernel
     W0 = cat_xp(f._coords, c)
     f.W_init_gpu.set(W0.astype(np.complex64))
     f.timeSteps = 2
