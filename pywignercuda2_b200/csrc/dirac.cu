@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(256, 2) k_dkinetic(Slots<C> S, DParams P, int 
 
 // potential sandwich on the (x, theta) grid: axis 0 theta_y, 1 y, 2 theta_x, 3 x
 template <class C>
-__global__ void __launch_bounds__(128, 3) k_dpotential(Slots<C> S, DParams P, DFactors<C> phase) {
+__global__ void __launch_bounds__(128, 4) k_dpotential(Slots<C> S, DParams P, DFactors<C> phase) {
     const long long n = (long long)P.n0 * P.n1 * P.n2 * P.n3;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         int i0, i1, i2, i3;
@@ -1009,7 +1009,7 @@ static int potential_impl(wigd_plan* p, void* const* slots, cudaStream_t st) {
     Slots<C> S;
     int r = make_slots(slots, S, true);
     if (r) return r;
-    k_dpotential<C><<<dgrid(p->npts, 128, 12), 128, 0, st>>>(S, p->P, phase_set<C>(p));
+    k_dpotential<C><<<dgrid(p->npts, 128, 16), 128, 0, st>>>(S, p->P, phase_set<C>(p));
     WIG_LAUNCHED("k_dpotential");
     return WIG_OK;
 }
