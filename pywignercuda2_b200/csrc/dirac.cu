@@ -600,7 +600,7 @@ __global__ void k_dfinalize(const double* __restrict__ part, int nblk, double dv
 // value_out = scale * S * DFT2(S * value_in), S = (-1)^(row+col), which is
 // the pair of FAFT calls for |delta| N = 1 with N/2 even.
 template <class C, int NA, int NB, int NT, int KIND, bool FWD>
-__global__ void __launch_bounds__(NT) k_dplane(Slots<C> S, int n0, int n1, int n2, int n3, double2 scale,
+__global__ void __launch_bounds__(NT) k_dplane(const __grid_constant__ Slots<C> S, int n0, int n1, int n2, int n3, double2 scale,
                                                const double* __restrict__ d_norm) {
     extern __shared__ __align__(16) unsigned char smraw[];
     C* s = reinterpret_cast<C*>(smraw);
@@ -653,7 +653,7 @@ struct DPlaneG {
     static constexpr int PSP = ((NA * LD + 13) / 16) * 16 + 2;   // plane stride, = 2 (mod 16)
 };
 template <class C, int NA, int NB, int NT, bool FWD, int G>
-__global__ void __launch_bounds__(NT) k_dplane_g(Slots<C> S, int n0, int n1, int n2, int n3, double2 scale,
+__global__ void __launch_bounds__(NT) k_dplane_g(const __grid_constant__ Slots<C> S, int n0, int n1, int n2, int n3, double2 scale,
                                                  const double* __restrict__ d_norm) {
     extern __shared__ __align__(16) unsigned char smraw[];
     constexpr int LD = NB + 1, PSP = DPlaneG<NA, LD>::PSP;

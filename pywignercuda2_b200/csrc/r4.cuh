@@ -1113,7 +1113,7 @@ template <class C> struct PlaneSlots { C* p[16]; };
 
 template <class C, int KIND, bool FWD>
 __global__ void __launch_bounds__(r4::NT, (sizeof(C) == 16 ? 2 : 4))
-k_dplane_r4(PlaneSlots<C> S, const C* __restrict__ gtw, double2 scale, const double* __restrict__ d_norm) {
+k_dplane_r4(const __grid_constant__ PlaneSlots<C> S, const C* __restrict__ gtw, double2 scale, const double* __restrict__ d_norm) {
     using namespace r4;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* s = reinterpret_cast<C*>(smraw);
