@@ -2,9 +2,11 @@
 
 Tolerances: complex128 (the drop-in) must match the oracle to 1e-12
 relative in norms and observables and 1e-10 in max|dW| / max|W|, the
-north-star bar.  complex64 (the precision form) is held to 1e-4 relative on
-the observables over the short runs here: its float32 state and transforms
-drift from the float64 result by about 1e-6 per step on these grids.
+north-star bar.  complex64 (the precision form) is held to about three
+times the error it reaches on each case (measured on B200): 2e-5 to 4e-5
+relative on the observables and 1e-6 to 3e-6 on the state against the
+oracle over these short runs, and below 1e-6 where two complex64 paths are
+compared with each other.
 """
 import ctypes
 
@@ -157,9 +159,9 @@ def test_run_precision_form_c64():
     p, c = config1(4, 32)
     init = lambda f, o: o.ho_ground(c[0], c[1], c[2], c[3], 1.0, 1.0, 1.0)
     f, Wo, obs = _run_both(p, init, 21, np.complex64)
-    for name in OBS:
+    for name in OBS:                          # reached: 4.1e-5 (observables), 2.8e-6 (state)
         assert rel_err(getattr(f, name), obs[name]) < 1e-4, name
-    assert rel_err(f.W_init_gpu.get(), Wo) < 1e-3
+    assert rel_err(f.W_init_gpu.get(), Wo) < 1e-5
 
 
 def test_run_cat_state_config2_prefix():
@@ -207,8 +209,8 @@ def test_run_fast64_vs_oracle():
     assert rel_err(f.W_init_gpu.get(), Wo) < 1e-10
 
 
-@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-12), (np.complex64, 1e-4)])
-def test_fast64_matches_generic_kernels(dtype, tol, monkeypatch):
+@pytest.mark.parametrize("dtype,tol,wtol", [(np.complex128, 1e-12, 1e-10), (np.complex64, 5e-5, 1e-5)])
+def test_fast64_matches_generic_kernels(dtype, tol, wtol, monkeypatch):
     from configs import cat_xp
     p, c = config2(3, 64)
     f1 = make_frame(GPU_Wigner4D, p, complex_dtype=dtype)
@@ -223,7 +225,7 @@ def test_fast64_matches_generic_kernels(dtype, tol, monkeypatch):
         f.Run()
     for name in OBS:
         assert rel_err(getattr(f1, name), getattr(f2, name)) < tol, name
-    assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < (100 * tol if tol < 1e-6 else 10 * tol)
+    assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < wtol      # complex64 reached 3.4e-6
 
 
 @pytest.mark.parametrize("n,dtype", [(32, np.complex128), (64, np.complex128), (64, np.complex64)])
@@ -271,16 +273,16 @@ def test_run_r4_c64_vs_oracle(kernel, monkeypatch):
     assert rel_err(f.W_init_gpu.get(), Wo) < 2e-5
 
 
-@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-12), (np.complex64, 1e-4)])
-def test_run_48_radix3_parity(dtype, tol):
+@pytest.mark.parametrize("dtype,tol,wtol", [(np.complex128, 1e-12, 1e-10), (np.complex64, 1e-4, 5e-6)])
+def test_run_48_radix3_parity(dtype, tol, wtol):
     """48 = 3 x 16 points per axis: fused half-steps with a radix-3 pass."""
     p, c = config1(5, 48)
     init = lambda f, o: o.ho_ground(c[0], c[1], c[2], c[3], 1.0, 1.0, 1.0) / np.pi ** 2
     f, Wo, obs = _run_both(p, init, 6, dtype)
     assert f._plan_fused() == (True, True)
-    for name in OBS:
+    for name in OBS:                          # complex64 reached 3.2e-5 (observables), 1.3e-6 (state)
         assert rel_err(getattr(f, name), obs[name]) < tol, name
-    assert rel_err(f.W_init_gpu.get(), Wo) < (1e-10 if tol < 1e-6 else 1e-3)
+    assert rel_err(f.W_init_gpu.get(), Wo) < wtol
 
 
 @pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-13), (np.complex64, 2e-5)])
@@ -351,7 +353,7 @@ def test_general_delta_fused_vs_oracle_32():
     assert rel_err(f.W_init_gpu.get(), Wo) < 1e-10
 
 
-@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-12), (np.complex64, 1e-4)])
+@pytest.mark.parametrize("dtype,tol", [(np.complex128, 1e-12), (np.complex64, 2e-6)])
 def test_general_delta_fused_matches_unfused_64(dtype, tol, monkeypatch):
     """k_dense_half against the unfused FAFT passes on the notebook windows at 64^4."""
     from configs import cat_xp
@@ -369,7 +371,8 @@ def test_general_delta_fused_matches_unfused_64(dtype, tol, monkeypatch):
         f.Run()
     for name in OBS:
         assert rel_err(getattr(f1, name), getattr(f2, name)) < tol, name
-    assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < (1e-10 if tol < 1e-6 else 1e-3)
+    # complex64 reached 6.2e-7 (observables) and 6.9e-7 (state)
+    assert rel_err(f1.W_init_gpu.get(), f2.W_init_gpu.get()) < (1e-10 if dtype == np.complex128 else 2e-6)
 
 
 @pytest.mark.parametrize("n", [32, 64])
