@@ -1183,6 +1183,14 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
         ::"r"(r4t::sa(dst)), "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(r4t::sa(bar))
         : "memory");
 }
+// issue and commit only (the issuing thread waits later, cp.async.bulk.wait_group.read)
+__device__ __forceinline__ void tma_store_4d_issue(const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                                   const void* src) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];"
+                 ::"l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(r4t::sa(src))
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
 __device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3, const void* src) {
     asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];"
                  ::"l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(r4t::sa(src))
@@ -1195,7 +1203,9 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, int c0, int
 template <class C>
 constexpr int dplane_gp() { return 16 / (int)sizeof(C); }
 template <class C>
-constexpr size_t dplane_r4t_smem_bytes() { return 128 + 65536 + 64 * sizeof(C) + 16 + 2 * 8 * 8 * sizeof(double); }
+constexpr size_t dplane_r4t_smem_bytes() {
+    return 128 + 65536 + 64 * sizeof(C) + 16 + 2 * 8 * 8 * sizeof(double) + 2 * 16 * sizeof(double);
+}
 
 // EPI (Theta -> P only): boundary_xp and Real_GPU of the diagonal on the
 // transformed values before they are stored (the same rounding as the
@@ -1270,6 +1280,13 @@ k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, const __grid_constant__ 
         dpt::tma_load_4d(s, map, 2 * GP * m, 0, i1, 0, bar);
     }
     load_tw(tw, gtw, threadIdx.x);
+    // EPI: the plane's constants (A0..A3, D1A0..D1A2 at (i1, i3), then x, y), read
+    // now so that their latency hides behind the copy and the transform
+    double* pconst = reinterpret_cast<double*>(bar + 2) + 2 * 64;
+    if (EPI && t < 9) {
+        const int i3c = GP * m + grp;
+        pconst[grp * 16 + t] = t < 7 ? E.obs_xy[t * 4096 + i1 * 64 + i3c] : (t == 7 ? E.cx[i3c] : E.cy[i1]);
+    }
     double2 sc = scale;
     if (d_norm) sc = zmul(sc, zinv(make_double2(d_norm[0], d_norm[1])));
     const C cc = to_c<C>(sc);
@@ -1320,6 +1337,15 @@ k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, const __grid_constant__ 
         const int slot = blockIdx.y, i3 = GP * m + grp;
         const bool diag = slot == 0 || slot == 5 || slot == 10 || slot == 15;
         const double m13 = E.mxp[3][i3], m11 = E.mxp[1][i1];
+        // this thread's four columns i2: held in registers for complex128; the
+        // complex64 kernel (64 registers) reads them per point
+        constexpr bool HOLD = sizeof(C) == 16;
+        double m2[4], pxj[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            m2[j] = HOLD ? E.mxp[2][c2 + 4 * c1 + 16 * j] : 0.0;
+            pxj[j] = HOLD ? E.cpx[c2 + 4 * c1 + 16 * j] : 0.0;
+        }
         double mo[depi::NM];
 #pragma unroll
         for (int q = 0; q < depi::NM; ++q) mo[q] = 0.0;
@@ -1331,12 +1357,12 @@ k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, const __grid_constant__ 
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int i2 = c2 + 4 * c1 + 16 * j;
-                const double r = E.mxp[2][i2] * m0 * m13 * m11;
+                const double r = (HOLD ? m2[j] : E.mxp[2][i2]) * m0 * m13 * m11;
                 const double2 d = to_d2(cmul(v[4 * i + j], ccs));   // the value a plain transform stores
                 C w = to_c<C>(make_double2(d.x * r, d.y * r));
                 if (diag) w.y = 0;
                 s[(i0 * 64 + i2) * GP + grp] = w;
-                const double px = E.cpx[i2], wr = (double)w.x, wi = (double)w.y;
+                const double px = HOLD ? pxj[j] : E.cpx[i2], wr = (double)w.x, wi = (double)w.y;
                 sr += wr; sx = fma(px, wr, sx); sx2 = fma(px * px, wr, sx2); si += wi;
             }
             mo[0] += sr; mo[1] += sx; mo[2] += sx2;
@@ -1353,7 +1379,11 @@ k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, const __grid_constant__ 
         if (l == 0)
 #pragma unroll
             for (int q = 0; q < depi::NM; ++q) red[w * 8 + q] = mo[q];
+        r4t::fence_async_smem();                       // generic-proxy writes visible to the tensor store
         __syncthreads();
+        // the store leaves first; each group's thread 0 then turns its plane's
+        // moments into the plane's row while the copy reads shared memory
+        if (threadIdx.x == 0) dpt::tma_store_4d_issue(map, 2 * GP * m, 0, i1, 0, s);
         if (t == 0) {
             double tot[depi::NM];
 #pragma unroll
@@ -1361,12 +1391,15 @@ k_dplane_r4t(const __grid_constant__ PlaneMaps<C> maps, const __grid_constant__ 
                 tot[q] = 0.0;
                 for (int ww = 0; ww < 8; ++ww) tot[q] += red[ww * 8 + q];
             }
-            const long long ixy = (long long)i1 * 64 + i3;
+            const double* pc = pconst + grp * 16;
             double A[7];
 #pragma unroll
-            for (int q = 0; q < 7; ++q) A[q] = E.obs_xy[q * 4096 + ixy];
-            depi::row(E, slot, E.cx[i3], E.cy[i1], A, tot, E.rows + ((long long)slot * 4096 + ixy) * DEPI_SUMS);
+            for (int q = 0; q < 7; ++q) A[q] = pc[q];
+            const long long ixy = (long long)i1 * 64 + i3;
+            depi::row(E, slot, pc[7], pc[8], A, tot, E.rows + ((long long)slot * 4096 + ixy) * DEPI_SUMS);
         }
+        if (threadIdx.x == 0) r4ring::bulk_wait_read();    // the copy has read the box before the CTA exits
+        return;
     }
     r4t::fence_async_smem();                           // generic-proxy writes visible to the tensor store
     __syncthreads();
