@@ -154,6 +154,44 @@ __device__ __forceinline__ void sandwich(const M4& L, double2 (&w)[16], const M4
         }
 }
 
+// The two halves of sandwich() in place, with the same sums in the same order:
+// w <- L w one column at a time, w <- w R one row at a time (four temporaries
+// each), so that a kernel can build R only after L has been applied.
+template <unsigned NZL>
+__device__ __forceinline__ void left_apply(const M4& L, double2 (&w)[16]) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        double2 col[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if ((NZL >> (4 * a + k)) & 1u) s = zadd(s, zmul(L.a[a][k], w[4 * k + b]));
+            col[a] = s;
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a) w[4 * a + b] = col[a];
+    }
+}
+template <unsigned NZR>
+__device__ __forceinline__ void right_apply(double2 (&w)[16], const M4& R) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        double2 row[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if ((NZR >> (4 * k + b)) & 1u) s = zadd(s, zmul(w[4 * a + k], R.a[k][b]));
+            row[b] = s;
+        }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) w[4 * a + b] = row[b];
+    }
+}
+
 // K11, K14 of the free Dirac propagator (GPU_WignerDirac4D.py:377-388)
 __device__ __forceinline__ void kin_entries(double px, double py, double m, double dt, const DParams& P,
                                             double2& k11, double2& k14) {
@@ -366,14 +404,22 @@ __global__ void __launch_bounds__(128, 4) k_dpotential(Slots<C> S, DParams P, DF
         decode(i, P, i0, i1, i2, i3);
         double2 w[16];
         load16(S, i, w);
-        const double A1m = a_field(P, 0, 0, i3, i2, i1, i0), A2m = a_field(P, 1, 0, i3, i2, i1, i0);
-        const double A3m = P.a3zero ? 0.0 : a_field(P, 2, 0, i3, i2, i1, i0);
-        const double A1p = a_field(P, 0, 1, i3, i2, i1, i0), A2p = a_field(P, 1, 1, i3, i2, i1, i0);
-        const double A3p = P.a3zero ? 0.0 : a_field(P, 2, 1, i3, i2, i1, i0);
-        const M4 UL = pot_matrix(A1m, A2m, A3m, P.dt, false, P);
-        const M4 UR = pot_matrix(A1p, A2p, A3p, P.kvn ? P.dt : -P.dt, true, P);
-        if (P.kvn || P.a3zero) sandwich<SPIN_NZ, SPIN_NZ>(UL, w, UR);
-        else sandwich<DPOT_NZ, DPOT_NZ>(UL, w, UR);
+        // UL W UR, UR built only after UL has been applied (fewer live registers)
+        const bool spin = P.kvn || P.a3zero;
+        {
+            const double A1m = a_field(P, 0, 0, i3, i2, i1, i0), A2m = a_field(P, 1, 0, i3, i2, i1, i0);
+            const double A3m = P.a3zero ? 0.0 : a_field(P, 2, 0, i3, i2, i1, i0);
+            const M4 UL = pot_matrix(A1m, A2m, A3m, P.dt, false, P);
+            if (spin) left_apply<SPIN_NZ>(UL, w);
+            else left_apply<DPOT_NZ>(UL, w);
+        }
+        {
+            const double A1p = a_field(P, 0, 1, i3, i2, i1, i0), A2p = a_field(P, 1, 1, i3, i2, i1, i0);
+            const double A3p = P.a3zero ? 0.0 : a_field(P, 2, 1, i3, i2, i1, i0);
+            const M4 UR = pot_matrix(A1p, A2p, A3p, P.kvn ? P.dt : -P.dt, true, P);
+            if (spin) right_apply<SPIN_NZ>(w, UR);
+            else right_apply<DPOT_NZ>(w, UR);
+        }
         const double2 ev = dfactor_at(phase, i0, i1, i2, i3, i);
 #pragma unroll
         for (int k = 0; k < 16; ++k) w[k] = zmul(w[k], ev);
