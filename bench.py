@@ -522,8 +522,7 @@ def main():
     state_bytes = P * 16
     kin_ms, pot_ms, fin_ms = [m / K for m in f.run_device_timed(f.W_init_gpu, K, hist)]
     run64 = f.plan_info()["run64_kernel"]
-    names = {"r4t": ("k_r4t<kin>", "k_r4t<pot>"), "r4": ("k_r4<kin>", "k_r4<pot>"),
-             "r4ring": ("k_r4ring<kin>", "k_r4ring<pot>"), "r4ring_ts": ("k_r4ring<kin>", "k_r4ring<pot>"),
+    names = {"r4": ("k_r4<kin>", "k_r4<pot>"), "r4ring_ts": ("k_r4ring<kin>", "k_r4ring<pot>"),
              "r4ring_pc": ("k_r4ring<kin>", "k_r4ring<pot>")}.get(run64, ("k_kinetic", "k_potential"))
     dom_name, dom_ms = (names[1], pot_ms) if pot_ms >= kin_ms else (names[0], kin_ms)
     peaks = _peaks()
@@ -643,7 +642,7 @@ def main():
             "precision_form": precision,
             "tensor_core_form": tensor_form,
             "mixed_form": mixed_form,
-            "gpu_launches": (4 * K + 4) if run64 in ("r4", "r4t", "r4ring", "r4ring_ts", "r4ring_pc") else (3 * K + 3),
+            "gpu_launches": (4 * K + 4) if run64 in ("r4", "r4ring_ts", "r4ring_pc") else (3 * K + 3),
             "finite": finite, "roofline": roofline, "clocks": clocks,
             "e2e": {"value": ws * K / (e2e_ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d / K,
                     "d2h_bytes_per_step": d2h / K,

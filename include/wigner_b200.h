@@ -263,11 +263,11 @@ int wig4d_observables_noalloc(const void* W, const int shape[4], int dtype,
 /* Which kernels a plan runs (no counterpart in the reference): info[0] fused
    kinetic half-step, info[1] fused potential half-step, info[2] the 64^4
    radix Run() kernels (1 or 0 each); info[3] the 64^4 Run() kernels: 0 none,
-   3 k_r4 (16 points per thread, the default), 4 k_r4t (complex128 k_r4 with
-   TMA plane loads, WIG_FAST64_KERNEL=r4t), 6 k_tc64 (tensor-core transforms,
+   3 k_r4 (16 points per thread: the complex64 default; complex128 with
+   WIG_FAST64_KERNEL=r4 or r4cluster), 6 k_tc64 (tensor-core transforms,
    wig4d_desc.transform = 1), 7 k_r4 with FP64 transforms on complex64
-   storage (wig4d_desc.transform = 3), 8 k_r4ring (complex128 persistent
-   k_r4 with a TMA ring of planes, WIG_FAST64_KERNEL=r4ring), 9 k_r4ring
+   storage (wig4d_desc.transform = 3 with WIG_MIXED_KERNEL=r4), 9 k_r4ring
+   (complex128 persistent ring of TMA-loaded planes) on the LA / LB layouts
    with TMA tensor stores (WIG_FAST64_KERNEL=r4ring_ts), 10 k_r4ring on the
    plane-contiguous layouts with bulk stores (the complex128 default), 11
    k_r4ring_mx (the mixed form of wig4d_desc.transform = 3 on the
@@ -281,15 +281,15 @@ int wig4d_plan_info(const wig4d_plan* plan, int info[4]);
  * kernel choices this plan has on a scratch copy of a Gaussian state
  * (`iterations` Run() iterations each, CUDA events on `stream`) and keeps
  * the fastest.  The candidates are the 64^4 engines (k_r4 with cluster or
- * plain stores, complex128 k_r4t and k_r4ring, and k_tc64 when the plan was made with
+ * plain stores, complex128 k_r4ring on either layout, and k_tc64 when the plan was made with
  * wig4d_desc.transform = 2) or, for the other kernels, k_kin48 against
  * k_kinetic on 48 x 48 planes and the columns per CTA of k_potential_g
  * (8, 4, 2, or k_potential).  The choice is cached per (shape, dtype,
  * kernel path) for the process: later plans with the same key take it
  * without timing unless flags has WIG_TUNE_FORCE.  choice_out (host, 4
  * ints, may be NULL) receives the engine (0 k_r4 plain, 1 k_r4 cluster,
- * 2 k_r4t, 3 k_tc64, 4 the per-size kernels, 5 k_r4ring, 6 k_r4ring with
- * TMA stores, 7 k_r4ring on plane-contiguous layouts), k_kin48 (1/0), the columns
+ * 3 k_tc64, 4 the per-size kernels, 6 k_r4ring on LA / LB with TMA stores,
+ * 7 k_r4ring on plane-contiguous layouts), k_kin48 (1/0), the columns
  * per CTA and the number of candidates timed.  Allocates a scratch state;
  * synchronous; call it outside any stream capture.
  */

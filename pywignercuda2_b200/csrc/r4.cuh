@@ -356,19 +356,9 @@ __global__ void k_from_r4_layout(const C* __restrict__ P, C* __restrict__ W, lon
 }
 
 // ---------------------------------------------------------------------------
-// k_r4t: the complex128 half-steps of k_r4 with the plane loaded by TMA.
-//
-// Same LA / LB layouts as k_r4 (IL = 2).  A plane of either half-step is,
-// in its source layout, 64 x 32 chunks of 32 bytes (two neighbouring points
-// of the fast in-plane axis) at strides of 128 KB and 4 MB, i.e. one 5-D
-// tensor box
-//   dims (innermost first)  (4 float64 = 2 points, f1, f0, c/2, r)
-//   box                     (4, 1, 1, 32, 64)
-// loaded with one cp.async.bulk.tensor (no multicast) into shared memory as
-// [r][c].  No thread issues a global load of the state; the copy completes
-// on an mbarrier whose wait is bounded: after the limit the CTA poisons the
-// norm (kinetic) or its partial row (potential) with NaN, so the run
-// reports a non-finite history, and returns.  Stores are those of k_r4.
+// TMA and mbarrier helpers of the persistent ring kernels and the Dirac plane
+// kernels: shared-memory addresses, mbarrier init / expect-tx / bounded waits,
+// and the 5-D tensor box load (cp.async.bulk.tensor, no multicast).
 // ---------------------------------------------------------------------------
 namespace r4t {
 
@@ -406,136 +396,6 @@ __device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, i
 
 }  // namespace r4t
 
-constexpr size_t r4t_smem_bytes() { return 128 + sizeof(double2) * (64 * 64 + 64) + 16; }
-
-template <bool KIN>
-__global__ void __launch_bounds__(r4::NT, 2)
-k_r4t(const __grid_constant__ CUtensorMap src_map, double2* __restrict__ dst,
-      const double2* __restrict__ PV, const double2* __restrict__ gtw, double2 scale, double* __restrict__ d_norm,
-      ObsTabs ob, double* __restrict__ partials) {
-    using namespace r4;
-    using namespace r4t;
-    typedef double2 C;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* s = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
-    C* tw = s + 64 * 64;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(tw + 64);
-    const int t = threadIdx.x, pl = blockIdx.x, f0 = pl >> 6, f1 = pl & 63;
-    const int ac = t & 15, ar = t >> 4;
-    if (t == 0) {
-        mbar_init(bar);
-        fence_async_smem();
-        mbar_expect_tx(bar, 64 * 64 * sizeof(C));
-        tma_load_5d(s, &src_map, 0, f1, f0, 0, 0, bar);
-    }
-    load_tw(tw, gtw, t);
-    double2 cc = scale;
-    if (KIN) cc = zmul(cc, zinv(make_double2(d_norm[0], d_norm[1])));
-    __syncthreads();                                   // barrier initialised before anyone waits
-    if (!mbar_wait_bounded(bar)) {
-        // the copy did not arrive: poison the results, wait once more (bounded)
-        // so that no copy still targets this CTA's shared memory, and leave
-        if (t == 0) {
-            if (KIN) d_norm[0] = __longlong_as_double(0x7ff8000000000000LL);
-            else partials[(long long)pl * NPART] = __longlong_as_double(0x7ff8000000000000LL);
-        }
-        mbar_wait_bounded(bar);
-        return;
-    }
-    const Lay L1 = lay1(t), L2 = lay2(t), L3 = lay3(t);
-    C v[16];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) v[4 * i + j] = s[(ar + 16 * i) * 64 + ac + 16 * j];
-    // ---- forward
-    pass<C, true>(v);
-    twiddle<C, true>(v, tw, ac, ar);
-    __syncthreads();                                   // the loaded plane has been read
-    put(s, L1, v);
-    __syncthreads();
-    get(s, L2, v);
-    pass<C, true>(v);
-    twiddle<C, true>(v, tw, 4 * (t & 3), 4 * ((t >> 4) & 3));
-    __syncthreads();
-    put(s, L2, v);
-    __syncthreads();
-    get(s, L3, v);
-    pass<C, true>(v);
-    {
-        const int c1 = t & 3, c2 = (t >> 2) & 3, r1 = (t >> 4) & 3, r2 = t >> 6;
-        const double2* pv = PV + (long long)pl * 128;
-        double2 b[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = __ldg(pv + 64 + c2 + 4 * c1 + 16 * j);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const double2 a = zmul(__ldg(pv + r2 + 4 * r1 + 16 * i), cc);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) factor_mul(v[4 * i + j], a, b[j]);
-        }
-    }
-    // ---- inverse
-    pass<C, false>(v);
-    twiddle<C, false>(v, tw, ((t >> 2) & 3) + 4 * (t & 3), (t >> 6) + 4 * ((t >> 4) & 3));
-    __syncthreads();
-    put(s, L3, v);
-    __syncthreads();
-    get(s, L2, v);
-    pass<C, false>(v);
-    twiddle<C, false>(v, tw, 4 * ((t >> 2) & 3), 4 * (t >> 6));
-    __syncthreads();
-    put(s, L2, v);
-    __syncthreads();
-    get(s, L1, v);
-    pass<C, false>(v);
-    if (!KIN) {
-        double a[NPART];
-#pragma unroll
-        for (int k = 0; k < NPART; ++k) a[k] = 0.0;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const double qy = __ldg(ob.cpy + ar + 16 * i);
-            double w0x = 0.0, w0y = 0.0;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const C w = v[4 * i + j];
-                const double qx = __ldg(ob.cpx + ac + 16 * j), k = __ldg(ob.ep + (ar + 16 * i) * 64 + ac + 16 * j);
-                w0x += w.x; w0y += w.y;
-                a[2] = fma(qx, w.x, a[2]); a[3] = fma(qx, w.y, a[3]);
-                a[4] = fma(qx * qx, w.x, a[4]); a[5] = fma(qx * qx, w.y, a[5]);
-                a[10] = fma(k, w.x, a[10]); a[11] = fma(k, w.y, a[11]);
-            }
-            a[0] += w0x; a[1] += w0y;
-            a[6] = fma(qy, w0x, a[6]); a[7] = fma(qy, w0y, a[7]);
-            a[8] = fma(qy * qy, w0x, a[8]); a[9] = fma(qy * qy, w0y, a[9]);
-        }
-        double* red = reinterpret_cast<double*>(s);
-        __syncthreads();                               // the last exchange has been read
-#pragma unroll
-        for (int k = 0; k < NPART; ++k) red[k * NT + t] = a[k];
-        __syncthreads();
-        const int w = t >> 5, l = t & 31;
-        for (int k = w; k < NPART; k += NT / 32) {
-            double sum = 0.0;
-#pragma unroll
-            for (int m = 0; m < NT / 32; ++m) sum += red[k * NT + m * 32 + l];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
-            if (l == 0) partials[(long long)pl * NPART + k] = sum;
-        }
-    }
-    // ---- store: point (r, c) = (ar + 16 i, ac + 16 j) into the destination layout
-    {
-        constexpr int IL = 2, NQ = 32;
-        C* g = dst + (((long long)f0 * NQ + f1 / IL) * 64 * 64 + ar * 64 + ac) * IL + (f1 % IL);
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) g[(i * 16 * 64 + j * 16) * IL] = v[4 * i + j];
-    }
-}
-
 // ---------------------------------------------------------------------------
 // k_r4ring: the 64^4 half-steps of k_r4 as a persistent kernel whose planes
 // stream through a ring of shared-memory buffers filled by TMA.
@@ -554,7 +414,7 @@ k_r4t(const __grid_constant__ CUtensorMap src_map, double2* __restrict__ dst,
 // observables and the stores from registers while the copy is in flight.
 // Every group's next plane has therefore been loading since the group
 // before it released a buffer, and no thread issues a global load of the
-// state.  A plane lands in natural [r][c] order (the box of k_r4t), is read
+// state.  A plane lands in natural [r][c] order, is read
 // straight into layout L1, and its buffer then serves as the exchange plane.
 // Exchanges and arithmetic are k_r4's, on one named barrier per group.
 //
@@ -655,20 +515,20 @@ __device__ __forceinline__ double warp_slot_sums(double (&a)[16], int lane) {
 
 }  // namespace r4ring
 
-// TS: the result leaves by one TMA tensor store per plane (dst_map, box
-// (2 reals, 1, 64, 64, 1) at (0, f1 % IL, 0, 0, unit)) from the plane's
-// buffer, written there in natural [r][c] order; the buffer's refill then
-// waits until the store has read it, which the group's thread 0 checks at
-// the group's next plane (after reading its input) or after its last plane.
-// Without TS each thread stores its 16 points (one IL-th of 16 sectors).
-// PC (with TS): the plane-contiguous layouts LK = [y][x][p_y][p_x] (kinetic
+// The result leaves by one copy per plane from the plane's buffer, written
+// there in natural [r][c] order; the buffer's refill then waits until the
+// copy has read it, which the group's thread 0 checks at the group's next
+// plane (after reading its input) or after its last plane.  On LA / LB the
+// copy is a TMA tensor store (dst_map, box (2 reals, 1, 64, 64, 1) at
+// (0, f1 % IL, 0, 0, unit)).
+// PC: the plane-contiguous layouts LK = [y][x][p_y][p_x] (kinetic
 // source, potential destination) and LP = [p_y][p_x][y][x] (the reverse).
 // Both half-steps then read point (r, c) of plane (f0, f1) at
 // src[((r * 64 + c) * 64 + f0) * 64 + f1] -- a box of one-point rows whose
 // sectors the other group's plane (f1 ^ 1) reads at the same time -- and
 // write the plane as one contiguous 64 KB block at dst + (f0 * 64 + f1) *
 // 4096 with a single bulk copy: whole lines, no partial-sector writes.
-template <class C, bool KIN, bool TS, bool PC = false>
+template <class C, bool KIN, bool PC>
 __global__ void __launch_bounds__(r4ring::Cfg<C>::NTH, 1)
 k_r4ring(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map,
          C* __restrict__ dst, const double2* __restrict__ PV, const C* __restrict__ gtw, double2 scale,
@@ -720,7 +580,7 @@ k_r4ring(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CU
             issued[b] += 1;
         }
     };
-    int pend = -1;                                     // TS, thread 0: plane whose buffer awaits its refill
+    int pend = -1;                                     // thread 0: plane whose buffer awaits its refill
     __syncthreads();                                   // barriers, counters and twiddles ready
     for (int k = g; k < nloc; k += NG) {
         const int bf = k % NB, pl = plane_of(k), f0 = pl >> 6, f1 = pl & 63;
@@ -746,7 +606,7 @@ k_r4ring(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CU
         pass<C, true>(v);
         twiddle<C, true>(v, tw, ac, ar);
         group_sync(g);                                 // the landed plane has been read
-        if (TS && t == 0 && pend >= 0) {
+        if (t == 0 && pend >= 0) {
             bulk_wait_read();                          // the previous plane's store has left its buffer
             refill(pend);
             pend = -1;
@@ -787,28 +647,20 @@ k_r4ring(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CU
         group_sync(g);
         get(s, L1, v);
         group_sync(g);                                 // the group's last exchange has been read
-        if (!TS && t == 0) refill(k);
         pass<C, false>(v);
-        if (TS) {
-            // ---- stage the plane as [r][c] and store it with one tensor copy
+        {
+            // ---- stage the plane as [r][c] and store it with one copy
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) s[(ar + 16 * i) * 64 + ac + 16 * j] = v[4 * i + j];
-            fence_async_smem();                        // generic-proxy writes visible to the tensor store
+            fence_async_smem();                        // generic-proxy writes visible to the copy engine
             group_sync(g);
             if (t == 0) {
                 if (PC) bulk_store_1d(dst + (long long)pl * 4096, s, (uint32_t)K::PLANE);
                 else tma_store_5d(&dst_map, 0, f1 % IL, 0, 0, f0 * NQ + f1 / IL, s);
                 pend = k;
             }
-        } else {
-            // ---- store: point (r, c) = (ar + 16 i, ac + 16 j), one IL-th of each sector
-            C* gd = dst + (((long long)f0 * NQ + f1 / IL) * 64 * 64 + ar * 64 + ac) * IL + (f1 % IL);
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) gd[(i * 16 * 64 + j * 16) * IL] = v[4 * i + j];
         }
         if (!KIN) {
             // observables of the new (x, p) state: p_y = ar + 16 i, p_x = ac + 16 j
@@ -847,7 +699,7 @@ k_r4ring(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CU
             }
         }
     }
-    if (TS && t == 0) {
+    if (t == 0) {
         if (pend >= 0) {
             bulk_wait_read();
             if (!*abort_word) refill(pend);            // another group may still need that plane
@@ -1084,7 +936,7 @@ k_r4ring_mx(const __grid_constant__ CUtensorMap src_map, float2* __restrict__ ds
     }
 }
 
-// The 64-entry twiddle table of k_r4 / k_r4t, built once per plan.
+// The 64-entry twiddle table of k_r4 and the ring kernels, built once per plan.
 template <class C>
 __global__ void k_make_r4_twiddles(C* tw) { r4::make_tw<C>(tw); }
 

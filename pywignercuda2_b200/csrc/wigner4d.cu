@@ -742,16 +742,13 @@ struct wig4d_plan {
     void* pingpong;                // second state buffer (layout [y][x][p_y][p_x])
     void* pv;                      // per-plane factor vectors of the two half-steps
     bool r4;                       // 64^4 Run(): k_r4 (16 points per thread) on its LA / LB layouts
-    bool r4t;                      // complex128 64^4 Run(): k_r4 with TMA plane loads (k_r4t)
     bool r4_cluster;               // k_r4 launched as clusters with full-sector stores
     bool kin48;                    // 48 x 48 kinetic planes: k_kin48 (else k_kinetic)
     int pot_gmax;                  // k_potential_g: at most this many columns per CTA (< 2: k_potential)
     bool tc_ready;                 // k_tc64's buffers exist (wig4d_desc.transform 1 or 2)
     int tuned;                     // wig4d_autotune has set the choices above
-    bool r4t_ready;                // k_r4t's tensor map and attributes are set
     bool r4ring;                   // complex128 64^4 Run(): persistent k_r4ring (TMA plane ring)
     bool r4ring_ready;             // k_r4ring's tensor map and attributes are set
-    bool r4ring_ts;                // k_r4ring with TMA tensor stores
     bool r4ring_pc;                // k_r4ring on the plane-contiguous layouts LK / LP (bulk stores)
     bool r4_mixed;                 // complex64 64^4: k_r4 with FP64 transforms on complex64 storage
     bool mx_ring;                  // the mixed form with k_r4ring_mx on the plane-contiguous layouts
@@ -1138,32 +1135,19 @@ static int ensure_w_maps(wig4d_plan* p, const void* W) {
     return WIG_OK;
 }
 
-// k_r4 with TMA plane loads (complex128): the LA map of the ping-pong buffer
-// (the LB map of the caller's state is made at the first run).
-static int ensure_r4t(wig4d_plan* p) {
-    if (p->r4t_ready) return WIG_OK;
-    int r;
-    if ((r = encode_plane_map(&p->map_t_load, p->pingpong))) return r;
-    WIG_CUDA(cudaFuncSetAttribute(k_r4t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4t_smem_bytes()));
-    WIG_CUDA(cudaFuncSetAttribute(k_r4t<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r4t_smem_bytes()));
-    p->r4t_ready = true;
-    return WIG_OK;
-}
-
-// k_r4ring (complex128): the same LA map of the ping-pong buffer as k_r4t.
+// k_r4ring (complex128): the LA / LK maps and the LA store map of the
+// ping-pong buffer (the caller's state gets its maps at the first run).
 static int ensure_r4ring(wig4d_plan* p) {
     if (p->r4ring_ready) return WIG_OK;
     int r;
-    if ((r = ensure_r4t(p))) return r;
+    if ((r = encode_plane_map(&p->map_t_load, p->pingpong))) return r;
     if ((r = encode_store_map(&p->map_t_store, p->pingpong))) return r;
     if ((r = encode_plane_map_pc(&p->map_t_load_pc, p->pingpong))) return r;
     const int sm = (int)r4ring::Cfg<double2>::SMEM;
-    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    WIG_CUDA(cudaFuncSetAttribute(k_r4ring<double2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
     p->r4ring_ready = true;
     return WIG_OK;
 }
@@ -1363,22 +1347,14 @@ extern "C" int wig4d_plan_create(const wig4d_desc* desc, wig4d_plan** out) {
         // complex128: k_r4ring on the plane-contiguous layouts (default);
         // complex64: k_r4 with cluster stores.  WIG_FAST64_KERNEL overrides: r4
         // (k_r4, plain stores), r4cluster (k_r4, cluster stores), and for
-        // complex128 r4t (TMA plane loads), r4ring (ring, per-thread stores),
-        // r4ring_ts (ring, TMA tensor stores on LA / LB), r4ring_pc
+        // complex128 r4ring_ts (the ring on LA / LB, TMA tensor stores), r4ring_pc
         const char* env_kern = getenv("WIG_FAST64_KERNEL");
         const char* kern = env_kern ? env_kern : (desc->dtype == WIG_C128 ? "r4ring_pc" : "r4cluster");
         p->r4 = true;
-        if (desc->dtype == WIG_C128 && strcmp(kern, "r4t") == 0) {
-            int r;
-            if ((r = ensure_r4t(p))) { free_plan(p); return r; }
-            p->r4t = true;
-        }
-        if (desc->dtype == WIG_C128 && (strcmp(kern, "r4ring") == 0 || strcmp(kern, "r4ring_ts") == 0 ||
-                                        strcmp(kern, "r4ring_pc") == 0)) {
+        if (desc->dtype == WIG_C128 && (strcmp(kern, "r4ring_ts") == 0 || strcmp(kern, "r4ring_pc") == 0)) {
             int r;
             if ((r = ensure_r4ring(p))) { free_plan(p); return r; }
             p->r4ring = true;
-            p->r4ring_ts = strcmp(kern, "r4ring") != 0;
             p->r4ring_pc = strcmp(kern, "r4ring_pc") == 0;
         }
         p->r4_cluster = strcmp(kern, "r4") != 0;
@@ -1500,7 +1476,7 @@ extern "C" int wig4d_plan_destroy(wig4d_plan* p) {
 extern "C" int wig4d_plan_info(const wig4d_plan* p, int info[4]) {
     if (!p || !info) return WIG_ERR_INVALID_ARG;
     info[0] = p->fused_kin; info[1] = p->fused_pot; info[2] = p->fast64;
-    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? (p->mx_ring ? 11 : 7) : p->mx_f32 ? 12 : (p->r4ring ? (p->r4ring_pc ? 10 : (p->r4ring_ts ? 9 : 8)) : (p->r4t ? 4 : 3))));
+    info[3] = p->tc ? 6 : (!p->fast64 ? 0 : (p->r4_mixed ? (p->mx_ring ? 11 : 7) : p->mx_f32 ? 12 : (p->r4ring ? (p->r4ring_pc ? 10 : 9) : 3)));
     return WIG_OK;
 }
 
@@ -1846,10 +1822,10 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
             if (p->r4ring_pc) {
                 // kinetic: LK (ping-pong) -> LP (W); potential: LP (W) -> LK (ping-pong)
                 if (part == 0)
-                    k_r4ring<double2, true, true, true><<<grid, K::NTH, K::SMEM, st>>>(
+                    k_r4ring<double2, true, true><<<grid, K::NTH, K::SMEM, st>>>(
                         p->map_t_load_pc, p->map_w_store, W, pv, tw, ks, p->cur_norm, p->ob, nullptr);
                 else if (part == 1)
-                    k_r4ring<double2, false, true, true><<<grid, K::NTH, K::SMEM, st>>>(
+                    k_r4ring<double2, false, true><<<grid, K::NTH, K::SMEM, st>>>(
                         p->map_w_load_pc, p->map_t_store, P, pvp, tw, ps, p->cur_norm, p->ob, p->partials);
                 else
                     return fold_and_finalize(p, hist, rows, st);
@@ -1857,43 +1833,13 @@ static int iteration_part(wig4d_plan* p, C* W, double* hist, int rows, cudaStrea
                 return WIG_OK;
             }
             if (part == 0) {
-                if (p->r4ring_ts)
-                    k_r4ring<double2, true, true><<<grid, K::NTH, K::SMEM, st>>>(p->map_t_load, p->map_w_store, W, pv,
-                                                                                 tw, ks, p->cur_norm, p->ob, nullptr);
-                else
-                    k_r4ring<double2, true, false><<<grid, K::NTH, K::SMEM, st>>>(p->map_t_load, p->map_w_store, W, pv,
-                                                                                  tw, ks, p->cur_norm, p->ob, nullptr);
+                k_r4ring<double2, true, false><<<grid, K::NTH, K::SMEM, st>>>(p->map_t_load, p->map_w_store, W, pv,
+                                                                              tw, ks, p->cur_norm, p->ob, nullptr);
                 WIG_LAUNCHED("k_r4ring<kin>");
             } else if (part == 1) {
-                if (p->r4ring_ts)
-                    k_r4ring<double2, false, true><<<grid, K::NTH, K::SMEM, st>>>(p->map_w_load, p->map_t_store, P, pvp,
-                                                                                  tw, ps, p->cur_norm, p->ob, p->partials);
-                else
-                    k_r4ring<double2, false, false><<<grid, K::NTH, K::SMEM, st>>>(p->map_w_load, p->map_t_store, P, pvp,
-                                                                                   tw, ps, p->cur_norm, p->ob, p->partials);
+                k_r4ring<double2, false, false><<<grid, K::NTH, K::SMEM, st>>>(p->map_w_load, p->map_t_store, P, pvp,
+                                                                               tw, ps, p->cur_norm, p->ob, p->partials);
                 WIG_LAUNCHED("k_r4ring<pot>");
-            } else {
-                return fold_and_finalize(p, hist, rows, st);
-            }
-            return WIG_OK;
-        }
-        if (p->r4t) {
-            int s;
-            if ((s = ensure_w_maps(p, W))) return s;
-            const double2* pv = reinterpret_cast<const double2*>(p->pv);
-            constexpr size_t sm = r4t_smem_bytes();
-            // kinetic: LA (ping-pong) -> LB (W); potential: LB (W) -> LA (ping-pong)
-            if (part == 0) {
-                k_r4t<true><<<64 * 64, r4::NT, sm, st>>>(p->map_t_load, W, pv, (const double2*)p->tw64,
-                                                         make_double2(p->kin_scale, 0.0), p->cur_norm, p->ob, nullptr);
-                WIG_LAUNCHED("k_r4t<kin>");
-            } else if (part == 1) {
-                k_r4t<false><<<64 * 64, r4::NT, sm, st>>>(p->map_w_load, reinterpret_cast<double2*>(p->pingpong),
-                                                          pv + (size_t)p->shape[0] * p->shape[2] * 128,
-                                                          (const double2*)p->tw64,
-                                                          make_double2(p->pot_scale, 0.0), p->cur_norm, p->ob,
-                                                          p->partials);
-                WIG_LAUNCHED("k_r4t<pot>");
             } else {
                 return fold_and_finalize(p, hist, rows, st);
             }
@@ -2118,23 +2064,17 @@ struct TuneKey {
 };
 struct TuneChoice { int engine, kin48, pot_gmax; };
 
-// engine: 0 k_r4 plain stores, 1 k_r4 cluster stores, 2 k_r4t, 3 k_tc64,
-// 4 the CUDA-core path of a plan without the 64^4 radix kernels, 5 k_r4ring,
-// 6 k_r4ring with TMA tensor stores, 7 k_r4ring on the plane-contiguous layouts
+// engine: 0 k_r4 plain stores, 1 k_r4 cluster stores, 3 k_tc64, 4 the
+// CUDA-core path of a plan without the 64^4 radix kernels, 6 k_r4ring on
+// LA / LB (TMA tensor stores), 7 k_r4ring on the plane-contiguous layouts
 int apply_choice(wig4d_plan* p, const TuneChoice& c) {
-    if (c.engine == 2) {
-        const int r = ensure_r4t(p);
-        if (r) return r;
-    }
-    if (c.engine >= 5 && c.engine <= 7) {
+    if (c.engine == 6 || c.engine == 7) {
         const int r = ensure_r4ring(p);
         if (r) return r;
     }
     p->tc = c.engine == 3;
     p->r4_cluster = c.engine == 1;
-    p->r4t = c.engine == 2;
-    p->r4ring = c.engine >= 5 && c.engine <= 7;
-    p->r4ring_ts = c.engine == 6 || c.engine == 7;
+    p->r4ring = c.engine == 6 || c.engine == 7;
     p->r4ring_pc = c.engine == 7;
     p->kin48 = c.kin48 != 0;
     p->pot_gmax = c.pot_gmax;
@@ -2144,7 +2084,7 @@ int apply_choice(wig4d_plan* p, const TuneChoice& c) {
 
 TuneChoice current_choice(const wig4d_plan* p) {
     TuneChoice c;
-    c.engine = p->tc ? 3 : (p->r4 ? (p->r4ring ? (p->r4ring_pc ? 7 : (p->r4ring_ts ? 6 : 5)) : (p->r4t ? 2 : (p->r4_cluster ? 1 : 0))) : 4);
+    c.engine = p->tc ? 3 : (p->r4 ? (p->r4ring ? (p->r4ring_pc ? 7 : 6) : (p->r4_cluster ? 1 : 0)) : 4);
     c.kin48 = p->kin48;
     c.pot_gmax = p->pot_gmax;
     return c;
@@ -2181,8 +2121,6 @@ extern "C" int wig4d_autotune(wig4d_plan* p, int iterations, int flags, void* st
     if (p->r4) {
         engines.push_back({1, base.kin48, base.pot_gmax});
         engines.push_back({0, base.kin48, base.pot_gmax});
-        if (p->dtype == WIG_C128) engines.push_back({2, base.kin48, base.pot_gmax});
-        if (p->dtype == WIG_C128) engines.push_back({5, base.kin48, base.pot_gmax});
         if (p->dtype == WIG_C128) engines.push_back({6, base.kin48, base.pot_gmax});
         if (p->dtype == WIG_C128) engines.push_back({7, base.kin48, base.pot_gmax});
     } else {

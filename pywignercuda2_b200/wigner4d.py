@@ -191,8 +191,8 @@ class GPU_Wigner4D:
         if self.autotune:
             ch = (ctypes.c_int * 4)()
             _lib.call("wig4d_autotune", plan, 3, 1 if self.autotune == "force" else 0, stream_ptr(), ch)
-            engines = {0: "k_r4 plain stores", 1: "k_r4 cluster stores", 2: "k_r4t", 3: "k_tc64",
-                       4: "per-size kernels", 5: "k_r4ring", 6: "k_r4ring TMA stores",
+            engines = {0: "k_r4 plain stores", 1: "k_r4 cluster stores", 3: "k_tc64",
+                       4: "per-size kernels", 6: "k_r4ring TMA stores",
                        7: "k_r4ring plane-contiguous"}
             self.autotune_choice = {"engine": engines[ch[0]], "k_kin48": bool(ch[1]), "pot_columns": ch[2],
                                     "timed": ch[3]}
@@ -346,7 +346,7 @@ class GPU_Wigner4D:
         """Kernels the plan runs: fused_kinetic, fused_potential, fast64, run64_kernel."""
         info = (ctypes.c_int * 4)()
         _lib.call("wig4d_plan_info", self._plan, info)
-        run64 = {0: None, 3: "r4", 4: "r4t", 6: "tc", 7: "r4_mixed", 8: "r4ring", 9: "r4ring_ts", 10: "r4ring_pc",
+        run64 = {0: None, 3: "r4", 6: "tc", 7: "r4_mixed", 9: "r4ring_ts", 10: "r4ring_pc",
                  11: "r4ring_mx", 12: "r4ring_f32"}[info[3]]
         return {"fused_kinetic": bool(info[0]), "fused_potential": bool(info[1]), "fast64": bool(info[2]),
                 "run64_kernel": run64}

@@ -310,13 +310,12 @@ def test_k48_matches_generic(dtype, tol, monkeypatch):
         assert rel_err(a, b) < tol
 
 
-@pytest.mark.parametrize("variant", ["r4t", "r4", "r4cluster", "r4ring", "r4ring_ts"])
+@pytest.mark.parametrize("variant", ["r4", "r4cluster", "r4ring_ts"])
 def test_r4_variants_match_default(variant, monkeypatch):
-    """complex128: k_r4 with TMA plane loads (r4t), k_r4 with plain (r4) or
-    cluster (r4cluster) stores, k_r4ring with per-thread stores (r4ring) or
-    TMA tensor stores (r4ring_ts) on LA / LB, against the default, k_r4ring
-    on the plane-contiguous layouts: the same arithmetic (the ring kernels
-    sum each plane's observables in another order)."""
+    """complex128: k_r4 with plain (r4) or cluster (r4cluster) stores and
+    k_r4ring on LA / LB with TMA tensor stores (r4ring_ts), against the
+    default, k_r4ring on the plane-contiguous layouts: the same arithmetic
+    (the ring kernels sum each plane's observables in another order)."""
     from configs import cat_xp
     p, c = config2(7, 64)
     f1 = make_frame(GPU_Wigner4D, p)
