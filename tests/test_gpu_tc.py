@@ -6,7 +6,7 @@ cores with operands split into fp16 hi + lo (about 22 significant bits,
 FP32 accumulation).  Measured against the complex128 form after 20
 iterations of the 64^4 cat state: energy 9e-5, <x> 8e-6, max|dW|/max|W|
 3e-5 relative; the tolerances below are three times those.  The complex128
-drop-in itself is held to the north-star bar (1e-12 observables, 1e-10
+drop-in itself is held to the parity bar (1e-12 observables, 1e-10
 state) against the NumPy oracle over the same 20 iterations.
 """
 import numpy as np

@@ -1,8 +1,8 @@
 """GPU parity of the scalar Wigner4D path against the NumPy oracle.
 
 Tolerances: complex128 (the drop-in) must match the oracle to 1e-12
-relative in norms and observables and 1e-10 in max|dW| / max|W|, the
-north-star bar.  complex64 (the precision form) is held to about three
+relative in norms and observables and 1e-10 in max|dW| / max|W| (the
+parity bar of the drop-in).  complex64 (the precision form) is held to about three
 times the error it reaches on each case (measured on B200): 2e-5 to 4e-5
 relative on the observables and 1e-6 to 3e-6 on the state against the
 oracle over these short runs, and below 1e-6 where two complex64 paths are
